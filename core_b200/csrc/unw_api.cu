@@ -1,0 +1,648 @@
+// Host orchestration and C ABI of the B200 unwrapper.
+//
+// A solve is: bounding box of valid pixels (one device->host read), per-grid
+// FFT plans and tables, setup + DCT initial solve, the IRLS loop (enqueued
+// `check_every` iterations at a time, then one small device->host read of the
+// per-grid state to see whether any grid is still iterating), and the device
+// post-processing.  All device memory comes from the caller's workspace; the
+// layout is computed by one function for both sizing and carving.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/unwrap_b200.h"
+#include "unw_kernels.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return set_err(UNW_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));  \
+    } while (0)
+
+constexpr int EMAX = 16;
+constexpr size_t ALIGN = 256;
+constexpr int HIST_CAP = 65536;
+constexpr int ELEM_MAX_CTAS = 1184;      // 8 x 148 SMs
+constexpr size_t COL_SMEM_BUDGET = 96 * 1024;
+constexpr int MAX_FFT = 16384;           // longest transform one CTA holds (1024 threads x 16)
+
+size_t up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// ------------------------------------------------------------ FFT plans
+bool smooth7(long long n) {
+    if (n < 1) return false;
+    for (int p : {2, 3, 5, 7})
+        while (n % p == 0) n /= p;
+    return n == 1;
+}
+long long next_smooth(long long x) {
+    while (!smooth7(x)) x++;
+    return x;
+}
+int fft_len(int N) { return smooth7(N) ? N : (int)next_smooth(2LL * N - 1); }
+
+std::vector<int> factor(int n) {
+    std::vector<int> r;
+    int m = n;
+    for (int p : {7, 5, 3})
+        while (m % p == 0) { r.push_back(p); m /= p; }
+    int twos = 0;
+    while (m % 2 == 0) { twos++; m /= 2; }
+    while (twos >= 4) { r.insert(r.begin(), 16); twos -= 4; }
+    if (twos == 3) r.insert(r.begin(), 8);
+    if (twos == 2) r.insert(r.begin(), 4);
+    if (twos == 1) r.insert(r.begin(), 2);
+    return r;
+}
+// complex elements one thread can hold per pass, over the radices of a plan
+int plan_cap(const std::vector<int>& rad) {
+    int c = EMAX;
+    for (int R : rad) c = std::min(c, (EMAX / R) * R);
+    return c;
+}
+int pick_threads(long long elems, int cap) {
+    for (int T : {128, 256, 512, 1024})
+        if ((long long)T * cap >= elems) return T;
+    return 0;
+}
+
+struct HostPlan {
+    int N = 0, n = 0, blue = 0, cap = 0;
+    std::vector<int> rad;
+};
+HostPlan make_plan(int N) {
+    HostPlan p;
+    p.N = N;
+    p.blue = smooth7(N) ? 0 : 1;
+    p.n = fft_len(N);
+    p.rad = p.n > 1 ? factor(p.n) : std::vector<int>{};
+    p.cap = plan_cap(p.rad);
+    return p;
+}
+
+// ------------------------------------------------------------ layout
+struct GridLayout {
+    size_t st, counter, part, tw_r, dw_r, ch_r, hs_r, cos_r, tw_c, dw_c, ch_c, hs_c, cos_c;
+    size_t arr[16];          // gx gy wx wy | wIx wIy b r z p0 p1 Ap T | U0 U1 Ub
+    size_t valid, hist, tilecnt;
+    size_t post_parent, post_lab, post_csum, post_ccount, post_remap, post_adj;
+    size_t end;
+    long long P0, max_ctas, lab_cap, ntiles_max;
+    int fr_cap, fc_cap;      // capacities of the FFT tables (row / column)
+};
+
+struct BatchLayout {
+    size_t rowany, colany, bbox, gdev, starts;
+    std::vector<size_t> base;
+    std::vector<GridLayout> g;
+    size_t total;
+};
+
+GridLayout grid_layout(long long H0, long long W0) {
+    GridLayout L{};
+    size_t o = 0;
+    auto take = [&](size_t bytes) { size_t r = o; o = up(o + bytes, ALIGN); return r; };
+    L.P0 = (long long)up((size_t)W0, 32);
+    const size_t A = (size_t)H0 * (size_t)L.P0 * sizeof(float);
+    L.max_ctas = std::max<long long>({(H0 + 1) / 2, (W0 + 1) / 2, ((W0 + 255) / 256) * H0, ELEM_MAX_CTAS});
+    L.fr_cap = (int)std::max<long long>(next_smooth(2 * W0 - 1), W0);
+    L.fc_cap = (int)std::max<long long>(next_smooth(2 * H0 - 1), H0);
+    L.st = take(sizeof(InstState));
+    L.counter = take(sizeof(unsigned) * 4);
+    L.part = take((size_t)L.max_ctas * UNW_NPART * sizeof(double));
+    L.tw_r = take(sizeof(float2) * L.fr_cap);
+    L.hs_r = take(sizeof(float2) * L.fr_cap);
+    L.dw_r = take(sizeof(float2) * W0);
+    L.ch_r = take(sizeof(float2) * W0);
+    L.cos_r = take(sizeof(double) * W0);
+    L.tw_c = take(sizeof(float2) * L.fc_cap);
+    L.hs_c = take(sizeof(float2) * L.fc_cap);
+    L.dw_c = take(sizeof(float2) * H0);
+    L.ch_c = take(sizeof(float2) * H0);
+    L.cos_c = take(sizeof(double) * H0);
+    for (int a = 0; a < 16; a++) L.arr[a] = take(A);
+    L.valid = take((size_t)H0 * L.P0);
+    L.hist = take(sizeof(int) * HIST_CAP);
+    L.ntiles_max = (H0 * W0 + 4095) / 4096;
+    L.tilecnt = take(sizeof(int) * (size_t)L.ntiles_max);
+    // post-processing scratch overlays the PCG arrays wIx..T (dead after the solve)
+    const long long npx = H0 * W0;
+    L.lab_cap = npx / 2 + 2;
+    size_t po = L.arr[4];
+    auto ptake = [&](size_t bytes) { size_t r = po; po = up(po + bytes, ALIGN); return r; };
+    L.post_parent = ptake(sizeof(int) * (size_t)npx);
+    L.post_lab = ptake(sizeof(int) * (size_t)npx);
+    L.post_csum = ptake(sizeof(double) * 4 * (size_t)L.lab_cap);
+    L.post_adj = ptake(sizeof(double) * (size_t)L.lab_cap);
+    L.post_ccount = ptake(sizeof(int) * (size_t)L.lab_cap);
+    L.post_remap = ptake(sizeof(int) * (size_t)L.lab_cap);
+    L.end = std::max(o, po);
+    return L;
+}
+
+BatchLayout batch_layout(int n, const long long* H, const long long* W) {
+    BatchLayout B;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { size_t r = o; o = up(o + bytes, ALIGN); return r; };
+    long long sh = 0, sw = 0;
+    for (int g = 0; g < n; g++) { sh += H[g]; sw += W[g]; }
+    B.rowany = take(sizeof(int) * (size_t)std::max(1LL, sh));
+    B.colany = take(sizeof(int) * (size_t)std::max(1LL, sw));
+    B.bbox = take(sizeof(int) * 4 * (size_t)n);
+    B.gdev = take(sizeof(GridDev) * (size_t)n);
+    B.starts = take(sizeof(int) * (size_t)KS_NKIND * (n + 1) + sizeof(int) * (n + 1));
+    for (int g = 0; g < n; g++) {
+        GridLayout L = grid_layout(H[g], W[g]);
+        B.base.push_back(o);
+        B.g.push_back(L);
+        o = up(o + L.end, ALIGN);
+    }
+    B.total = o + ALIGN;  // slack for aligning the caller's base pointer
+    return B;
+}
+
+// ------------------------------------------------------------ launch shapes
+struct Shape {
+    int row_T = 0, col_T = 0;
+    size_t row_smem = 0, col_smem = 0;
+};
+
+int elem_ctas(long long npx) {
+    long long c = (npx + 2047) / 2048;
+    return (int)std::max<long long>(1, std::min<long long>(c, ELEM_MAX_CTAS));
+}
+
+struct Solver {
+    int n = 0;
+    cudaStream_t s = nullptr;
+    std::vector<GridDev> hg;     // host copies
+    std::vector<int> starts;     // [KS_NKIND + 1][n + 1]  (last row: post tiles)
+    std::vector<int> total;      // CTAs per kind
+    GridDev* dg = nullptr;
+    int* dstarts = nullptr;
+    Shape sh;
+    UnwScalars sc{};
+    const int* ds(int kind) const { return dstarts + (size_t)kind * (n + 1); }
+};
+
+int kind_ctas(const GridDev& G, int kind) {
+    if (G.H == 0) return 0;
+    const long long npx = (long long)G.H * G.W;
+    switch (kind) {
+        case KS_ROWPAIR: return (G.H + 1) / 2;
+        case KS_COL: return (G.W + 2 * G.col_nseq - 1) / (2 * G.col_nseq);
+        case KS_STEN: return G.sten_tiles_x * ((G.H + G.sten_rows - 1) / G.sten_rows);
+        case KS_ELEM: return elem_ctas(npx);
+        case KS_ONE: return 1;
+        default: return (int)((npx + 4095) / 4096);  // post tiles
+    }
+}
+
+// ------------------------------------------------------------ IRLS enqueue
+int enqueue_iteration(Solver& S, int t) {
+    const int n = S.n;
+    cudaStream_t s = S.s;
+    CK(unw_launch_simple(UNW_K_MEAN, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
+    CK(unw_launch_simple(UNW_K_HEAD, S.total[KS_STEN], s, S.dg, S.ds(KS_STEN), n, t, S.sc));
+    CK(unw_launch_simple(UNW_K_COPY_BEST, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
+    CK(unw_launch_row_fwd(1, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, t, 0));
+    CK(unw_launch_col(1, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
+    CK(unw_launch_row_inv(1, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
+    for (int k = 0; k < S.sc.cg_max_iter; k++) {
+        CK(unw_launch_simple(UNW_K_MATVEC, S.total[KS_STEN], s, S.dg, S.ds(KS_STEN), n, k, S.sc));
+        CK(unw_launch_row_fwd(2, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, t, k));
+        CK(unw_launch_col(1, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
+        CK(unw_launch_row_inv(2, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
+    }
+    CK(unw_launch_simple(UNW_K_REL, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
+    return UNW_OK;
+}
+
+int read_states(Solver& S, std::vector<InstState>& out) {
+    out.resize(S.n);
+    for (int g = 0; g < S.n; g++)
+        CK(cudaMemcpyAsync(&out[g], S.hg[g].st, sizeof(InstState), cudaMemcpyDeviceToHost, S.s));
+    CK(cudaStreamSynchronize(S.s));
+    return UNW_OK;
+}
+
+int validate_params(const unw_params* p) {
+    if (!p) return set_err(UNW_E_ARG, "params is NULL");
+    if (p->max_iter < 0 || p->cg_max_iter < 0) return set_err(UNW_E_ARG, "negative iteration count");
+    return UNW_OK;
+}
+
+// Per-grid descriptors, FFT plans, launch shapes, CTA prefix arrays and
+// tables for grids cropped to bbox (r0, r1, c0, c1 per grid).
+int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbox, const unw_params* prm,
+            char* base, const BatchLayout& B, cudaStream_t s, bool dense) {
+    const std::vector<long long> H0 = [&] { std::vector<long long> v(n); for (int g = 0; g < n; g++) v[g] = grids[g].H; return v; }();
+    const std::vector<long long> W0 = [&] { std::vector<long long> v(n); for (int g = 0; g < n; g++) v[g] = grids[g].W; return v; }();
+    S.n = n;
+    S.s = s;
+    S.hg.resize(n);
+    S.sc.max_iter = prm->max_iter;
+    S.sc.cg_max_iter = prm->cg_max_iter;
+    S.sc.tol = prm->tol;
+    S.sc.cg_tol = prm->cg_tol;
+    S.sc.eps2 = (float)((double)prm->epsilon * (double)prm->epsilon);
+    S.sc.conncomp_size = prm->conncomp_size;
+    std::vector<HostPlan> prow(n), pcol(n);
+    for (int g = 0; g < n; g++) {
+        const unw_grid& q = grids[g];
+        const GridLayout& L = B.g[g];
+        char* gb = base + B.base[g];
+        GridDev& G = S.hg[g];
+        memset(&G, 0, sizeof(G));
+        const int r0 = bbox[4 * g], r1 = bbox[4 * g + 1], c0 = bbox[4 * g + 2], c1 = bbox[4 * g + 3];
+        G.H0 = (int)H0[g];
+        G.W0 = (int)W0[g];
+        G.H = r1 - r0;
+        G.W = c1 - c0;
+        G.r0 = r0;
+        G.c0 = c0;
+        G.P = dense ? G.W : (int)up((size_t)std::max(G.W, 1), 32);
+        G.phase = q.phase + (long long)r0 * q.phase_pitch + c0;
+        G.phase_pitch = q.phase_pitch;
+        G.weight = q.weight ? q.weight + (long long)r0 * q.weight_pitch + c0 : nullptr;
+        G.weight_pitch = q.weight_pitch;
+        G.out_u = q.out_u;
+        G.out_u_pitch = q.out_u_pitch;
+        G.out_cc = q.out_cc;
+        G.out_cc_pitch = q.out_cc_pitch;
+        G.congruent = (prm->flags & UNW_F_CONGRUENT) ? 1 : 0;
+        G.st = (InstState*)(gb + L.st);
+        G.counter = (unsigned*)(gb + L.counter);
+        G.part = (double*)(gb + L.part);
+        float** arrs[16] = {&G.gx, &G.gy, &G.wx, &G.wy, &G.wIx, &G.wIy, &G.b, &G.r,
+                            &G.z, &G.p0, &G.p1, &G.Ap, &G.T, &G.U0, &G.U1, &G.Ub};
+        for (int a = 0; a < 16; a++) *arrs[a] = (float*)(gb + L.arr[a]);
+        G.valid = (uint8_t*)(gb + L.valid);
+        G.cosH = (const double*)(gb + L.cos_c);
+        G.cosW = (const double*)(gb + L.cos_r);
+        G.hist = (int*)(gb + L.hist);
+        G.hist_cap = HIST_CAP;
+        G.tilecnt = (int*)(gb + L.tilecnt);
+        G.parent = (int*)(gb + L.post_parent);
+        G.lab = (int*)(gb + L.post_lab);
+        G.csum = (double*)(gb + L.post_csum);
+        G.adj = (double*)(gb + L.post_adj);
+        G.ccount = (int*)(gb + L.post_ccount);
+        G.remap = (int*)(gb + L.post_remap);
+        G.lab_cap = (int)std::min<long long>(L.lab_cap, (long long)G.H * G.W / 2 + 2);
+        G.ntiles = (int)(((long long)G.H * G.W + 4095) / 4096);
+        if (G.H == 0) continue;
+        prow[g] = make_plan(G.W);
+        pcol[g] = make_plan(G.H);
+        const HostPlan* pl[2] = {&prow[g], &pcol[g]};
+        DctPlanDev* dp[2] = {&G.prow, &G.pcol};
+        size_t tw[2] = {L.tw_r, L.tw_c}, hs[2] = {L.hs_r, L.hs_c}, dw[2] = {L.dw_r, L.dw_c},
+               ch[2] = {L.ch_r, L.ch_c};
+        int capn[2] = {L.fr_cap, L.fc_cap};
+        for (int d = 0; d < 2; d++) {
+            const HostPlan& hp = *pl[d];
+            if (hp.n > MAX_FFT || hp.n > capn[d] || (int)hp.rad.size() > UNW_MAX_PASSES)
+                return set_err(UNW_E_UNSUPPORTED, "grid %d: transform length %d (from %d) exceeds %d", g, hp.n,
+                               hp.N, MAX_FFT);
+            DctPlanDev& D = *dp[d];
+            D.N = hp.N;
+            D.blue = hp.blue;
+            D.stride = hp.n;
+            D.fft.n = hp.n;
+            D.fft.npass = (int)hp.rad.size();
+            for (size_t i = 0; i < hp.rad.size(); i++) D.fft.radix[i] = hp.rad[i];
+            D.fft.tw = (const float2*)(gb + tw[d]);
+            D.dctw = (const float2*)(gb + dw[d]);
+            D.chirp = (const float2*)(gb + ch[d]);
+            D.hspec = (const float2*)(gb + hs[d]);
+        }
+        // row kernel: one complex sequence (two rows) of fft_len(W)
+        const int rT = pick_threads(prow[g].n, prow[g].cap);
+        // column kernel: nseq column pairs of fft_len(H) under the shared-memory budget
+        int nseq = (int)std::max<size_t>(1, std::min<size_t>(8, COL_SMEM_BUDGET / ((size_t)pcol[g].n * sizeof(float2))));
+        nseq = std::min(nseq, (G.W + 1) / 2);
+        int cT = 0;
+        while (nseq >= 1 && !(cT = pick_threads((long long)nseq * pcol[g].n, pcol[g].cap))) nseq--;
+        if (!rT || !cT) return set_err(UNW_E_UNSUPPORTED, "grid %d: no launch shape", g);
+        G.col_nseq = nseq;
+        S.sh.row_T = std::max(S.sh.row_T, rT);
+        S.sh.col_T = std::max(S.sh.col_T, cT);
+        S.sh.row_smem = std::max(S.sh.row_smem, (size_t)prow[g].n * sizeof(float2));
+        S.sh.col_smem = std::max(S.sh.col_smem, (size_t)nseq * pcol[g].n * sizeof(float2));
+        G.sten_tiles_x = (G.W + 255) / 256;
+        G.sten_rows = (int)std::max<long long>(1, std::min<long long>(32, (long long)G.sten_tiles_x * G.H / 592));
+    }
+    // CTA prefix arrays
+    S.starts.assign((size_t)(KS_NKIND + 1) * (n + 1), 0);
+    S.total.assign(KS_NKIND + 1, 0);
+    for (int k = 0; k <= KS_NKIND; k++) {
+        int acc = 0;
+        for (int g = 0; g < n; g++) {
+            S.starts[(size_t)k * (n + 1) + g] = acc;
+            acc += kind_ctas(S.hg[g], k);
+        }
+        S.starts[(size_t)k * (n + 1) + n] = acc;
+        S.total[k] = acc;
+    }
+    S.dg = (GridDev*)(base + B.gdev);
+    S.dstarts = (int*)(base + B.starts);
+    CK(cudaMemcpyAsync(S.dg, S.hg.data(), sizeof(GridDev) * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(S.dstarts, S.starts.data(), sizeof(int) * S.starts.size(), cudaMemcpyHostToDevice, s));
+
+    // tables
+    for (int g = 0; g < n; g++) {
+        GridDev& G = S.hg[g];
+        if (G.H == 0) continue;
+        CK(unw_launch_tables(G.prow.fft, G.prow, const_cast<double*>(G.cosW), G.W, s));
+        CK(unw_launch_tables(G.pcol.fft, G.pcol, const_cast<double*>(G.cosH), G.H, s));
+        if (G.prow.blue) CK(unw_launch_hspec(pick_threads(prow[g].n, prow[g].cap), EMAX, G.prow, s));
+        if (G.pcol.blue) CK(unw_launch_hspec(pick_threads(pcol[g].n, pcol[g].cap), EMAX, G.pcol, s));
+        CK(cudaMemsetAsync(G.hist, 0, sizeof(int) * HIST_CAP, s));
+    }
+
+    return UNW_OK;
+}
+
+// ------------------------------------------------------------ batch solve
+int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, size_t ws_bytes,
+                unw_stats* stats, cudaStream_t s) {
+    if (n <= 0 || !grids) return set_err(UNW_E_ARG, "empty batch");
+    int rc = validate_params(prm);
+    if (rc) return rc;
+    std::vector<long long> H0(n), W0(n);
+    for (int g = 0; g < n; g++) {
+        const unw_grid& q = grids[g];
+        if (!q.phase || !q.out_u || !q.out_cc) return set_err(UNW_E_ARG, "grid %d: null pointer", g);
+        if (q.H <= 0 || q.W <= 0) return set_err(UNW_E_ARG, "grid %d: bad shape %lld x %lld", g, q.H, q.W);
+        if (q.H * q.W >= (1LL << 31)) return set_err(UNW_E_UNSUPPORTED, "grid %d: too many pixels", g);
+        if (q.phase_pitch < q.W || q.out_u_pitch < q.W || q.out_cc_pitch < q.W ||
+            (q.weight && q.weight_pitch < q.W))
+            return set_err(UNW_E_ARG, "grid %d: pitch smaller than width", g);
+        H0[g] = q.H;
+        W0[g] = q.W;
+    }
+    BatchLayout B = batch_layout(n, H0.data(), W0.data());
+    if (!ws) return set_err(UNW_E_ARG, "workspace is NULL");
+    char* base = (char*)up((size_t)ws, ALIGN);
+    if ((size_t)(base - (char*)ws) + B.total - ALIGN > ws_bytes)
+        return set_err(UNW_E_WORKSPACE, "workspace %zu bytes < %zu needed", ws_bytes, B.total);
+
+    // 1. bounding boxes
+    int* rowany = (int*)(base + B.rowany);
+    int* colany = (int*)(base + B.colany);
+    int* dbbox = (int*)(base + B.bbox);
+    {
+        long long ro = 0, co = 0;
+        for (int g = 0; g < n; g++) {
+            CK(unw_launch_bbox(grids[g].phase, grids[g].phase_pitch, (int)H0[g], (int)W0[g], rowany + ro,
+                               colany + co, dbbox + 4 * g, s));
+            ro += H0[g];
+            co += W0[g];
+        }
+    }
+    std::vector<int> bbox(4 * n);
+    CK(cudaMemcpyAsync(bbox.data(), dbbox, sizeof(int) * 4 * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+
+    Solver S;
+    rc = prepare(S, n, grids, bbox, prm, base, B, s, false);
+    if (rc) return rc;
+
+    // 4. setup and DCT initial solve (utils_unwrap2d.py:1228-1513)
+    const int tot_active = S.total[KS_ROWPAIR];
+    CK(unw_launch_simple(UNW_K_STATE_INIT, 1, s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
+    if (tot_active > 0) {
+        CK(unw_launch_simple(UNW_K_SETUP, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
+        CK(unw_launch_row_fwd(0, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, 0, 0));
+        CK(unw_launch_col(0, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
+        CK(unw_launch_row_inv(0, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
+        CK(unw_launch_simple(UNW_K_INIT_RECENTRE, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
+
+        // 5. IRLS loop (utils_unwrap2d.py:1533-1626)
+        const int every = std::max(1, prm->check_every);
+        std::vector<InstState> hs;
+        for (int t = 0; t < prm->max_iter; t++) {
+            rc = enqueue_iteration(S, t);
+            if (rc) return rc;
+            if ((t + 1) % every == 0 || t + 1 == prm->max_iter) {
+                rc = read_states(S, hs);
+                if (rc) return rc;
+                bool any = false;
+                for (int g = 0; g < n; g++) any |= (S.hg[g].H > 0 && hs[g].irls_active);
+                if (!any) break;
+            }
+        }
+
+        // 6. post-processing (utils_unwrap2d.py:1659-1757)
+        CK(unw_launch_post(UNW_P_KSTATS, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        CK(unw_launch_post(UNW_P_HIST, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        CK(unw_launch_post(UNW_P_MEDIAN, n, s, S.dg, nullptr, n, S.sc, S.hg.data()));
+        CK(unw_launch_post(UNW_P_SHIFT_CCINIT, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        CK(unw_launch_post(UNW_P_UNION, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        CK(unw_launch_post(UNW_P_FLATTEN, S.total[KS_NKIND], s, S.dg, S.ds(KS_NKIND), n, S.sc, S.hg.data()));
+        CK(unw_launch_post(UNW_P_TILESCAN, n, s, S.dg, nullptr, n, S.sc, S.hg.data()));
+        CK(unw_launch_post(UNW_P_LABEL, S.total[KS_NKIND], s, S.dg, S.ds(KS_NKIND), n, S.sc, S.hg.data()));
+        CK(unw_launch_post(UNW_P_ACCUM, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        CK(unw_launch_post(UNW_P_ADJUST, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        // size-ranked relabel (utils_unwrap2d.py:1722-1746): sizes to the host, sorted there
+        rc = read_states(S, hs);
+        if (rc) return rc;
+        for (int g = 0; g < n; g++) {
+            const GridDev& G = S.hg[g];
+            if (G.H == 0 || hs[g].n_nonfinite || !hs[g].hist_ok) continue;
+            const int nl = hs[g].n_labels;
+            std::vector<int> cnt(nl + 1);
+            CK(cudaMemcpyAsync(cnt.data(), G.ccount, sizeof(int) * (nl + 1), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            std::vector<int> order(nl);
+            std::iota(order.begin(), order.end(), 1);
+            std::sort(order.begin(), order.end(), [&](int a, int b) {
+                return cnt[a] != cnt[b] ? cnt[a] > cnt[b] : a > b;  // size desc; ties larger label first
+            });
+            std::vector<int> remap(nl + 1, 0);
+            int nw = 1;
+            for (int L : order)
+                if (cnt[L] >= prm->conncomp_size) remap[L] = nw++;
+            if (nw - 1 > 65535)
+                return set_err(UNW_E_OVERFLOW, "grid %d: %d components do not fit uint16 labels", g, nw - 1);
+            CK(cudaMemcpyAsync(G.remap, remap.data(), sizeof(int) * (nl + 1), cudaMemcpyHostToDevice, s));
+            if (stats) stats[g].n_components = nw - 1;
+        }
+        CK(unw_launch_post(UNW_P_WRITE, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+    }
+    CK(unw_launch_post(UNW_P_FILL, 0, s, S.dg, nullptr, n, S.sc, S.hg.data()));
+    std::vector<InstState> fin;
+    rc = read_states(S, fin);
+    if (rc) return rc;
+    int ret = UNW_OK;
+    for (int g = 0; g < n; g++) {
+        const GridDev& G = S.hg[g];
+        const InstState& st = fin[g];
+        int status = 0;
+        if (G.H == 0) status |= UNW_S_ALL_NAN;
+        else {
+            status = st.status;
+            if (st.n_nonfinite) { status |= UNW_S_NONFINITE_OUT; ret = UNW_W_NUMERIC; }
+            else if (!st.hist_ok) return set_err(UNW_E_UNSUPPORTED, "grid %d: post-processing limits exceeded", g);
+        }
+        if (stats) {
+            unw_stats& o = stats[g];
+            const int ncomp = o.n_components;
+            memset(&o, 0, sizeof(o));
+            o.n_components = (G.H > 0 && !st.n_nonfinite) ? ncomp : 0;
+            o.irls_iters = G.H ? st.irls_iter : 0;
+            o.cg_iters_total = G.H ? st.cg_total : 0;
+            o.cg_iters_last = (G.H && st.irls_iter > 0 && st.irls_iter <= UNW_MAX_LOG) ? st.cg_log[st.irls_iter - 1] : 0;
+            o.n_labels = G.H ? st.n_labels : 0;
+            o.status = status;
+            o.bbox[0] = bbox[4 * g]; o.bbox[1] = bbox[4 * g + 1]; o.bbox[2] = bbox[4 * g + 2]; o.bbox[3] = bbox[4 * g + 3];
+            o.rel_change = st.rel_change;
+            o.best_residual = st.best_residual;
+            o.k_median = st.kmed;
+            for (int i = 0; i < 64 && i < UNW_MAX_LOG; i++) o.cg_iters[i] = G.H ? st.cg_log[i] : 0;
+        }
+    }
+    return ret;
+}
+
+// Full-grid, dense-pitch descriptor over caller arrays for the operator entry points.
+int op_prepare(Solver& S, int64_t H, int64_t W, void* ws, size_t wsb, cudaStream_t s, const float* phase,
+               const float* weight) {
+    if (H <= 0 || W <= 0) return set_err(UNW_E_ARG, "bad shape %lld x %lld", (long long)H, (long long)W);
+    if (!ws) return set_err(UNW_E_ARG, "workspace is NULL");
+    long long h = H, w = W;
+    BatchLayout B = batch_layout(1, &h, &w);
+    char* base = (char*)up((size_t)ws, ALIGN);
+    if ((size_t)(base - (char*)ws) + B.total - ALIGN > wsb)
+        return set_err(UNW_E_WORKSPACE, "workspace %zu bytes < %zu needed", wsb, B.total);
+    unw_grid q{};
+    q.phase = phase;
+    q.phase_pitch = W;
+    q.weight = weight;
+    q.weight_pitch = W;
+    q.H = H;
+    q.W = W;
+    unw_params prm{};
+    prm.epsilon = 1e-2f;
+    std::vector<int> bbox = {0, (int)H, 0, (int)W};
+    return prepare(S, 1, &q, bbox, &prm, base, B, s, true);
+}
+
+int op_upload(Solver& S) {
+    CK(cudaMemcpyAsync(S.dg, S.hg.data(), sizeof(GridDev), cudaMemcpyHostToDevice, S.s));
+    return UNW_OK;
+}
+
+}  // namespace
+
+// ================================================================== C ABI
+extern "C" {
+
+int unw_abi_version(void) { return UNW_ABI_VERSION; }
+
+const char* unw_last_error(void) { return g_err.c_str(); }
+
+size_t unw_batch_workspace_bytes(int32_t n, const int64_t* H, const int64_t* W) {
+    if (n <= 0 || !H || !W) return 0;
+    std::vector<long long> h(n), w(n);
+    for (int g = 0; g < n; g++) {
+        if (H[g] <= 0 || W[g] <= 0) return 0;
+        h[g] = H[g];
+        w[g] = W[g];
+    }
+    return batch_layout(n, h.data(), w.data()).total;
+}
+
+size_t unw_workspace_bytes(int64_t H, int64_t W) { return unw_batch_workspace_bytes(1, &H, &W); }
+
+int unw_solve_f32(const float* phase, int64_t phase_pitch, const float* weight, int64_t weight_pitch,
+                  int64_t H, int64_t W, const unw_params* params, float* out_u, int64_t out_u_pitch,
+                  uint16_t* out_cc, int64_t out_cc_pitch, void* workspace, size_t workspace_bytes,
+                  unw_stats* stats, void* cuda_stream) {
+    unw_grid g;
+    g.phase = phase;
+    g.phase_pitch = phase_pitch;
+    g.weight = weight;
+    g.weight_pitch = weight_pitch;
+    g.H = H;
+    g.W = W;
+    g.out_u = out_u;
+    g.out_u_pitch = out_u_pitch;
+    g.out_cc = out_cc;
+    g.out_cc_pitch = out_cc_pitch;
+    return solve_batch(1, &g, params, workspace, workspace_bytes, stats, (cudaStream_t)cuda_stream);
+}
+
+int unw_solve_batch(int32_t n, const unw_grid* grids, const unw_params* params, void* workspace,
+                    size_t workspace_bytes, unw_stats* stats, void* cuda_stream) {
+    return solve_batch(n, grids, params, workspace, workspace_bytes, stats, (cudaStream_t)cuda_stream);
+}
+
+int unw_setup_gradients(const float* phase, const float* weight, int64_t H, int64_t W, float* gx, float* gy,
+                        float* wx, float* wy, uint8_t* valid, void* workspace, size_t workspace_bytes,
+                        void* cuda_stream) {
+    if (!phase || !gx || !gy || !wx || !wy || !valid) return set_err(UNW_E_ARG, "null pointer");
+    Solver S;
+    int rc = op_prepare(S, H, W, workspace, workspace_bytes, (cudaStream_t)cuda_stream, phase, weight);
+    if (rc) return rc;
+    GridDev& G = S.hg[0];
+    G.gx = gx; G.gy = gy; G.wx = wx; G.wy = wy; G.valid = valid;
+    rc = op_upload(S);
+    if (rc) return rc;
+    CK(unw_launch_simple(UNW_K_STATE_INIT, 1, S.s, S.dg, S.ds(KS_ELEM), 1, 0, S.sc));
+    CK(unw_launch_simple(UNW_K_SETUP, S.total[KS_ELEM], S.s, S.dg, S.ds(KS_ELEM), 1, 0, S.sc));
+    return UNW_OK;
+}
+
+int unw_apply_laplacian(const float* x, const float* wx, const float* wy, int64_t H, int64_t W, float* Ax,
+                        void* workspace, size_t workspace_bytes, void* cuda_stream) {
+    if (!x || !wx || !wy || !Ax) return set_err(UNW_E_ARG, "null pointer");
+    Solver S;
+    int rc = op_prepare(S, H, W, workspace, workspace_bytes, (cudaStream_t)cuda_stream, nullptr, nullptr);
+    if (rc) return rc;
+    GridDev& G = S.hg[0];
+    G.r = const_cast<float*>(x); G.wIx = const_cast<float*>(wx); G.wIy = const_cast<float*>(wy); G.Ap = Ax;
+    rc = op_upload(S);
+    if (rc) return rc;
+    CK(unw_launch_simple(UNW_K_LAP_APPLY, S.total[KS_ELEM], S.s, S.dg, S.ds(KS_ELEM), 1, 0, S.sc));
+    return UNW_OK;
+}
+
+int unw_apply_preconditioner(const float* r, int64_t H, int64_t W, float* z, void* workspace,
+                             size_t workspace_bytes, void* cuda_stream) {
+    if (!r || !z) return set_err(UNW_E_ARG, "null pointer");
+    Solver S;
+    int rc = op_prepare(S, H, W, workspace, workspace_bytes, (cudaStream_t)cuda_stream, nullptr, nullptr);
+    if (rc) return rc;
+    GridDev& G = S.hg[0];
+    G.r = const_cast<float*>(r); G.z = z;
+    rc = op_upload(S);
+    if (rc) return rc;
+    CK(unw_launch_row_fwd(3, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg, S.ds(KS_ROWPAIR), 1, 0, 0));
+    CK(unw_launch_col(0, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, S.s, S.dg, S.ds(KS_COL), 1));
+    CK(unw_launch_row_inv(3, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg, S.ds(KS_ROWPAIR), 1));
+    return UNW_OK;
+}
+
+}  // extern "C"

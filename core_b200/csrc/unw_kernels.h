@@ -1,0 +1,60 @@
+// Host-side declarations of the kernel launchers (implemented in the .cu files).
+#pragma once
+#include <cuda_runtime.h>
+#include "unw_internal.cuh"
+
+struct UnwScalars {
+    int max_iter;
+    int cg_max_iter;
+    float tol;
+    float cg_tol;
+    float eps2;
+    int conncomp_size;
+};
+
+enum {
+    UNW_K_STATE_INIT = 0,
+    UNW_K_SETUP,
+    UNW_K_MATVEC,
+    UNW_K_HEAD,
+    UNW_K_MEAN,
+    UNW_K_INIT_RECENTRE,
+    UNW_K_COPY_BEST,
+    UNW_K_REL,
+    UNW_K_LAP_APPLY
+};
+
+// solver kernels
+cudaError_t unw_launch_tables(const FftPlanDev& f, const DctPlanDev& d, double* cosv, int Ncos,
+                              cudaStream_t s);
+cudaError_t unw_launch_hspec(int T, int emax, const DctPlanDev& d, cudaStream_t s);
+cudaError_t unw_launch_row_fwd(int mode, int T, int emax, int nblk, size_t smem, cudaStream_t s,
+                               const GridDev* gd, const int* starts, int n, int it, int cgk);
+cudaError_t unw_launch_row_inv(int mode, int T, int emax, int nblk, size_t smem, cudaStream_t s,
+                               const GridDev* gd, const int* starts, int n);
+cudaError_t unw_launch_col(int mode, int T, int emax, int nblk, size_t smem, cudaStream_t s,
+                           const GridDev* gd, const int* starts, int n);
+cudaError_t unw_launch_simple(int which, int nblk, cudaStream_t s, const GridDev* gd,
+                              const int* starts, int n, int it, UnwScalars sc);
+
+// bounding box of valid pixels on the caller's full grid
+cudaError_t unw_launch_bbox(const float* phase, long long pitch, int H0, int W0, int* rowany,
+                            int* colany, int* bbox, cudaStream_t s);
+
+// post-processing
+enum {
+    UNW_P_KSTATS = 0,   // non-finite count, min/max cycle count
+    UNW_P_HIST,         // histogram of cycle counts
+    UNW_P_MEDIAN,       // median -> shift (one CTA per grid)
+    UNW_P_SHIFT_CCINIT, // apply shift, NaN restore, union-find init
+    UNW_P_UNION,        // union with right/down neighbours
+    UNW_P_FLATTEN,      // root per pixel, roots per tile
+    UNW_P_TILESCAN,     // exclusive scan of tile counts (one CTA per grid)
+    UNW_P_LABEL,        // compact labels of roots
+    UNW_P_ACCUM,        // per-label sin/cos sums and counts
+    UNW_P_ADJUST,       // per-label circular-mean adjustment
+    UNW_P_WRITE,        // outputs into the caller's full grid
+    UNW_P_FILL          // NaN / 0 outside the crop and for failed grids
+};
+cudaError_t unw_launch_post(int which, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
+                            int n, const UnwScalars& sc, const GridDev* host_grids);

@@ -1,0 +1,797 @@
+// Solver kernels of the B200 DCT+IRLS unwrapper (sm_100a).
+//
+// One IRLS iteration (utils_unwrap2d.py:1533-1626) is the launch sequence
+//   mean -> head -> copy_best -> row_fwd(R0) -> col -> row_inv(Z0)
+//   -> cg_max_iter x [matvec -> row_fwd(UPD) -> col -> row_inv(Z)] -> rel
+// Every kernel covers all grids of a batch and returns at once for grids whose
+// IRLS or PCG has stopped; the stop decisions (the reference's Python `break`
+// tests) are taken on the device by the last CTA of the reducing kernel, so
+// no host synchronisation is needed inside an IRLS iteration.
+//
+// The DCT preconditioner (utils_unwrap2d.py:1390-1403) is three passes:
+//   row_fwd: row DCT-II of a pair of rows through one complex FFT,
+//   col:     column DCT-II -> scale by -1/lambda -> column DCT-III (fused),
+//   row_inv: row DCT-III of a pair of rows through one complex FFT,
+// each pass fused with the elementwise PCG work that reads or writes the
+// same rows.  Float32 elementwise arithmetic follows the reference's
+// operation order (one rounding per torch op); all inner products and norms
+// accumulate in float64.
+#include <climits>
+#include "unw_fft.cuh"
+#include "unw_kernels.h"
+
+// ============================================================ tables
+// Twiddles, DCT weights and Bluestein chirps in float64, rounded once.
+__global__ void k_tables(FftPlanDev f, DctPlanDev d, double* cosv, int Ncos) {
+    float2* tw = const_cast<float2*>(f.tw);
+    float2* dw = const_cast<float2*>(d.dctw);
+    float2* ch = const_cast<float2*>(d.chirp);
+    const int n = f.n, N = d.N;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+        double s, c;
+        sincospi(-2.0 * (double)m / (double)n, &s, &c);
+        tw[m] = make_float2((float)c, (float)s);
+    }
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+        double s, c;
+        sincospi(-(double)k / (2.0 * (double)N), &s, &c);
+        dw[k] = make_float2((float)c, (float)s);
+        if (d.blue) {
+            long long m2 = ((long long)k * (long long)k) % (2LL * N);
+            sincospi((double)m2 / (double)N, &s, &c);
+            ch[k] = make_float2((float)c, (float)s);
+        }
+    }
+    // cos(pi*i/N) for the Neumann-Laplacian eigenvalues (utils_unwrap2d.py:1284-1289)
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Ncos; k += gridDim.x * blockDim.x)
+        cosv[k] = cospi((double)k / (double)Ncos);
+}
+
+// Bluestein filter spectrum hspec = FFT_M(h) / M, h_j = chirp_|j| for |j| < N.
+template <int T, int EMAX>
+__global__ void __launch_bounds__(T) k_hspec(DctPlanDev d) {
+    extern __shared__ float2 sm[];
+    const int M = d.fft.n, N = d.N;
+    for (int m = threadIdx.x; m < M; m += T) {
+        float2 v = make_float2(0.f, 0.f);
+        if (m < N) v = d.chirp[m];
+        else if (M - m < N) v = d.chirp[M - m];
+        sm[m] = v;
+    }
+    __syncthreads();
+    fft_smem<T, EMAX>(sm, 1, M, d.fft);
+    float2* hs = const_cast<float2*>(d.hspec);
+    const float inv = 1.0f / (float)M;
+    for (int m = threadIdx.x; m < M; m += T) hs[m] = make_float2(sm[m].x * inv, sm[m].y * inv);
+}
+
+// ============================================================ state / setup
+__global__ void k_state_init(const GridDev* __restrict__ grids, int n, UnwScalars sc) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    InstState* s = grids[g].st;
+    s->rz = 0; s->pAp = 0; s->rnorm = 0; s->alpha = 0.f; s->beta = 0.f;
+    s->cg_active = 0; s->cg_iter = 0; s->pfirst = 1;
+    s->irls_active = sc.max_iter > 0; s->irls_iter = 0; s->max_iter = sc.max_iter;
+    s->best_update = 0; s->revert = 0; s->u_index = 0; s->status = 0;
+    s->vcount = 0; s->mean = 0; s->residual = 0; s->best_residual = INFINITY; s->rel_change = 0;
+    s->tol = sc.tol; s->cg_tol = sc.cg_tol; s->eps2 = sc.eps2; s->cg_max_iter = sc.cg_max_iter;
+    s->cg_total = 0;
+    for (int i = 0; i < UNW_MAX_LOG; i++) s->cg_log[i] = 0;
+    s->n_nonfinite = 0; s->kmin = INT_MAX; s->kmax = INT_MIN; s->hist_ok = 1; s->kmed = 0.f; s->shift = 0.f;
+    s->n_labels = 0;
+    if (grids[g].H == 0) { s->irls_active = 0; s->hist_ok = 0; }
+    *grids[g].counter = 0u;
+}
+
+// NaN fill, weight clipping, wrapped gradients and edge weights
+// (utils_unwrap2d.py:1228-1241, :1254-1262, :1267-1275).  KS_ELEM shape.
+__device__ __forceinline__ float wrap_f(float d) { return atan2f(sinf(d), cosf(d)); }
+
+__device__ __forceinline__ void px_in(const GridDev& G, int i, int j, float& ph, float& w, bool& v) {
+    const float p = G.phase[(long long)i * G.phase_pitch + j];
+    v = !isnan(p);
+    ph = v ? p : 0.f;
+    if (G.weight) {
+        float x = G.weight[(long long)i * G.weight_pitch + j];
+        if (isnan(x) || !v) x = 0.f;
+        w = fminf(fmaxf(x, 0.01f), 1.0f);
+    } else {
+        w = v ? 1.f : 0.f;
+    }
+}
+
+__global__ void k_setup(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
+    __shared__ double red[32 * 1];
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int H = G.H, W = G.W, P = G.P;
+    const long long npx = (long long)H * W;
+    double acc[1] = {0.0};
+    for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
+        const int i = (int)(q / W), j = (int)(q - (long long)i * W);
+        float ph, w, phr, wr, phd, wd;
+        bool v, vr, vd;
+        px_in(G, i, j, ph, w, v);
+        float gxv = 0.f, wxv = 0.f, gyv = 0.f, wyv = 0.f;
+        if (j < W - 1) {
+            px_in(G, i, j + 1, phr, wr, vr);
+            gxv = wrap_f(fsub(phr, ph));
+            wxv = fmul(fdiv(fadd(w, wr), 2.0f), (v && vr) ? 1.f : 0.f);
+        }
+        if (i < H - 1) {
+            px_in(G, i + 1, j, phd, wd, vd);
+            gyv = wrap_f(fsub(phd, ph));
+            wyv = fmul(fdiv(fadd(w, wd), 2.0f), (v && vd) ? 1.f : 0.f);
+        }
+        const size_t o = (size_t)i * P + j;
+        G.gx[o] = gxv; G.gy[o] = gyv; G.wx[o] = wxv; G.wy[o] = wyv;
+        G.valid[o] = v ? 1 : 0;
+        acc[0] += v ? 1.0 : 0.0;
+    }
+    if (arrive<1>(G, local, nct, acc, red)) {
+        finish_sum<1>(G, nct, acc, red);
+        if (threadIdx.x == 0) G.st->vcount = acc[0];
+    }
+}
+
+// ============================================================ Laplacian helpers
+// A x at (i, j): -div(w grad x) in the reference's op order (utils_unwrap2d.py:1367-1388):
+// res = 0; res -= dx[j-1]; res += dx[j]; res -= dy[i-1]; res += dy[i]; Ax = -res.
+__device__ __forceinline__ float lap_at(const float* __restrict__ x, const float* __restrict__ wx,
+                                        const float* __restrict__ wy, int i, int j, int H, int W, int P) {
+    const size_t o = (size_t)i * P + j;
+    const float xc = x[o];
+    float res = 0.f;
+    if (j > 0) res = fsub(res, fmul(fsub(xc, x[o - 1]), wx[o - 1]));
+    if (j < W - 1) res = fadd(res, fmul(fsub(x[o + 1], xc), wx[o]));
+    if (i > 0) res = fsub(res, fmul(fsub(xc, x[o - P]), wy[o - P]));
+    if (i < H - 1) res = fadd(res, fmul(fsub(x[o + P], xc), wy[o]));
+    return -res;
+}
+
+// ============================================================ row forward pass
+// Row DCT-II of rows (i0, i0+1) of a source computed on the fly.
+// MODE 0 (RHO):  rho = -div(w g), the DCT initial solve (utils_unwrap2d.py:1478-1483)
+// MODE 1 (R0):   r = b - A x0, PCG start (utils_unwrap2d.py:1413-1419)
+// MODE 2 (UPD):  x += alpha p; r -= alpha Ap (utils_unwrap2d.py:1445-1459)
+// Output T[i][k] = 2 * DCT-II(row i)[k] / 2 (unnormalised, no 1/2 factor).
+template <int MODE>
+__device__ __forceinline__ bool rowfwd_gate(const InstState* s) {
+    if (MODE == 0 || MODE == 3) return true;
+    if (MODE == 1) return s->irls_active != 0;
+    return s->irls_active != 0 && s->cg_active != 0;
+}
+
+template <int T, int EMAX, int MODE>
+__global__ void __launch_bounds__(T) k_row_fwd(const GridDev* __restrict__ grids,
+                                               const int* __restrict__ starts, int n, int it,
+                                               int cgk) {
+    extern __shared__ float2 sm[];
+    __shared__ double red[32 * 2];
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    InstState* st = G.st;
+    if (!rowfwd_gate<MODE>(st)) return;
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int H = G.H, W = G.W, P = G.P;
+    const int i0 = 2 * local, i1 = i0 + 1;
+    const bool has1 = i1 < H;
+    double acc[2] = {0.0, 0.0};
+    float* U = (it & 1) ? G.U0 : G.U1;  // x of this IRLS iteration (U_nxt)
+    const float* pk = (MODE == 2) ? ((cgk & 1) ? G.p1 : G.p0) : nullptr;
+    const float alpha = (MODE == 2) ? st->alpha : 0.f;
+    for (int j = threadIdx.x; j < W; j += T) {
+        float a = 0.f, b = 0.f;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int i = i0 + h;
+            if (h == 1 && !has1) break;
+            const size_t o = (size_t)i * P + j;
+            float val;
+            if (MODE == 0) {
+                float rr = 0.f;
+                if (j > 0) rr = fadd(rr, fmul(G.wx[o - 1], G.gx[o - 1]));
+                if (j < W - 1) rr = fsub(rr, fmul(G.wx[o], G.gx[o]));
+                if (i > 0) rr = fadd(rr, fmul(G.wy[o - P], G.gy[o - P]));
+                if (i < H - 1) rr = fsub(rr, fmul(G.wy[o], G.gy[o]));
+                val = rr;
+            } else if (MODE == 3) {
+                val = G.r[o];
+            } else if (MODE == 1) {
+                const float ax = lap_at(U, G.wIx, G.wIy, i, j, H, W, P);
+                val = fsub(G.b[o], ax);
+                G.r[o] = val;
+                acc[0] += isfinite(val) ? 0.0 : 1.0;
+            } else {
+                const float xn = fmaf(alpha, pk[o], U[o]);
+                const float rn = fmaf(-alpha, G.Ap[o], G.r[o]);
+                U[o] = xn;
+                G.r[o] = rn;
+                acc[0] += (double)rn * (double)rn;
+                acc[1] += isfinite(xn) ? 0.0 : 1.0;
+                val = rn;
+            }
+            if (h == 0) a = val; else b = val;
+        }
+        sm[mk_perm(j, W)] = make_float2(a, b);
+    }
+    __syncthreads();
+    dft_n<T, EMAX>(sm, 1, G.prow);
+    // Two real rows from one complex DFT, then X_k = Re(exp(-i pi k/2W) V_k).
+    const float2* __restrict__ dw = G.prow.dctw;
+    for (int k = threadIdx.x; k < W; k += T) {
+        const float2 C = sm[k];
+        const float2 Cm = sm[k == 0 ? 0 : W - k];
+        const float2 Va = make_float2(C.x + Cm.x, C.y - Cm.y);
+        const float2 Vb = make_float2(C.y + Cm.y, Cm.x - C.x);
+        const float2 w = __ldg(&dw[k]);
+        G.T[(size_t)i0 * P + k] = w.x * Va.x - w.y * Va.y;
+        if (has1) G.T[(size_t)i1 * P + k] = w.x * Vb.x - w.y * Vb.y;
+    }
+    if (MODE == 0 || MODE == 3) return;
+    if (arrive<2>(G, local, nct, acc, red)) {
+        finish_sum<2>(G, nct, acc, red);
+        if (threadIdx.x == 0) {
+            if (MODE == 1) {
+                // non-finite initial residual: CG returns x0 (utils_unwrap2d.py:1418-1419)
+                st->cg_active = acc[0] == 0.0 ? 1 : 0;
+            } else {
+                const double rn = sqrt(acc[0]);
+                st->rnorm = rn;
+                if (acc[1] != 0.0 || !(rn >= (double)st->cg_tol) || !isfinite(rn)) st->cg_active = 0;
+            }
+        }
+    }
+}
+
+// ============================================================ column pass
+// Column DCT-II -> scale by -1/(4 H W lambda) -> column DCT-III, in place on T.
+// MODE 0: DCT initial solve (always runs); MODE 1: PCG (gated).
+template <int T, int EMAX, int MODE>
+__global__ void __launch_bounds__(T) k_col(const GridDev* __restrict__ grids,
+                                           const int* __restrict__ starts, int n) {
+    extern __shared__ float2 sm[];
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    const InstState* st = G.st;
+    if (MODE == 1 && !(st->irls_active && st->cg_active)) return;
+    const int local = blockIdx.x - starts[g];
+    const int H = G.H, W = G.W, P = G.P;
+    const int c0 = 2 * G.col_nseq * local;
+    const int nseq = min(G.col_nseq, (W - c0 + 1) >> 1);
+    const DctPlanDev& PC = G.pcol;
+    const int sd = PC.stride;
+    float* __restrict__ Tm = G.T;
+    for (int q = threadIdx.x; q < nseq * H; q += T) {
+        const int i = q / nseq, s = q - i * nseq;
+        const int c = c0 + 2 * s;
+        const float a = Tm[(size_t)i * P + c];
+        const float b = (c + 1 < W) ? Tm[(size_t)i * P + c + 1] : 0.f;
+        sm[s * sd + mk_perm(i, H)] = make_float2(a, b);
+    }
+    __syncthreads();
+    dft_n<T, EMAX>(sm, nseq, PC);
+    const float2* __restrict__ dw = PC.dctw;
+    const double* __restrict__ cH = G.cosH;
+    const double* __restrict__ cW = G.cosW;
+    const float negs = -1.0f / (4.0f * (float)H * (float)W);
+    const int nh = H / 2 + 1;
+    for (int q = threadIdx.x; q < nseq * nh; q += T) {
+        const int k = q / nseq, s = q - k * nseq;
+        const int km = k == 0 ? 0 : H - k;
+        if (k > km) continue;
+        float2* base = sm + s * sd;
+        const float2 C = base[k], Cm = base[km];
+        const int ja = c0 + 2 * s, jb = ja + 1;
+        // DCT-II of the two columns at frequencies k and km
+        const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
+        const float2 Vak = make_float2(C.x + Cm.x, C.y - Cm.y);
+        const float2 Vbk = make_float2(C.y + Cm.y, Cm.x - C.x);
+        const float2 Vam = make_float2(Cm.x + C.x, Cm.y - C.y);
+        const float2 Vbm = make_float2(Cm.y + C.y, C.x - Cm.x);
+        float Xak = wk.x * Vak.x - wk.y * Vak.y, Xbk = wk.x * Vbk.x - wk.y * Vbk.y;
+        float Xam = wm.x * Vam.x - wm.y * Vam.y, Xbm = wm.x * Vbm.x - wm.y * Vbm.y;
+        // divide by the Neumann-Laplacian eigenvalue, negate, zero the DC term
+        const double ck = cH[k], cm = cH[km];
+        const double ca = cW[ja], cb = jb < W ? cW[jb] : 1.0;
+        const float lak = (float)(2.0 * ck + 2.0 * ca - 4.0), lbk = (float)(2.0 * ck + 2.0 * cb - 4.0);
+        const float lam = (float)(2.0 * cm + 2.0 * ca - 4.0), lbm = (float)(2.0 * cm + 2.0 * cb - 4.0);
+        Xak = (k == 0 && ja == 0) ? 0.f : fdiv(Xak, lak) * negs;
+        Xam = (km == 0 && ja == 0) ? 0.f : fdiv(Xam, lam) * negs;
+        Xbk = jb < W ? fdiv(Xbk, lbk) * negs : 0.f;
+        Xbm = jb < W ? fdiv(Xbm, lbm) * negs : 0.f;
+        // DCT-III pre-twiddle: V'_k = conj(w_k) (Y_k - i Y_{H-k}), Y_H = 0; store conj(C')
+        const float mak = k == 0 ? 0.f : Xam, mbk = k == 0 ? 0.f : Xbm;
+        const float2 Pak = cmul(cconj(wk), make_float2(Xak, -mak));
+        const float2 Pbk = cmul(cconj(wk), make_float2(Xbk, -mbk));
+        base[k] = cconj(make_float2(Pak.x - Pbk.y, Pak.y + Pbk.x));
+        if (km != k) {
+            const float2 Pam = cmul(cconj(wm), make_float2(Xam, -Xak));
+            const float2 Pbm = cmul(cconj(wm), make_float2(Xbm, -Xbk));
+            base[km] = cconj(make_float2(Pam.x - Pbm.y, Pam.y + Pbm.x));
+        }
+    }
+    __syncthreads();
+    dft_n<T, EMAX>(sm, nseq, PC);
+    for (int q = threadIdx.x; q < nseq * H; q += T) {
+        const int i = q / nseq, s = q - i * nseq;
+        const int c = c0 + 2 * s;
+        const float2 v = sm[s * sd + mk_perm(i, H)];
+        Tm[(size_t)i * P + c] = v.x;
+        if (c + 1 < W) Tm[(size_t)i * P + c + 1] = -v.y;
+    }
+}
+
+// ============================================================ row inverse pass
+// Row DCT-III of rows (i0, i0+1) of T, with the epilogue:
+// MODE 0 (INITU): u = nan_to_num(z) (utils_unwrap2d.py:1498-1502), sum over valid pixels
+// MODE 1 (Z0):    z = M^-1 r, rz = r.z                (utils_unwrap2d.py:1421-1428)
+// MODE 2 (Z):     z = M^-1 r, beta from r.z          (utils_unwrap2d.py:1461-1472)
+template <int MODE>
+__device__ __forceinline__ bool rowinv_gate(const InstState* s) {
+    if (MODE == 0 || MODE == 3) return true;
+    return s->irls_active != 0 && s->cg_active != 0;
+}
+
+template <int T, int EMAX, int MODE>
+__global__ void __launch_bounds__(T) k_row_inv(const GridDev* __restrict__ grids,
+                                               const int* __restrict__ starts, int n) {
+    extern __shared__ float2 sm[];
+    __shared__ double red[32 * 2];
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    InstState* st = G.st;
+    if (!rowinv_gate<MODE>(st)) return;
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int H = G.H, W = G.W, P = G.P;
+    const int i0 = 2 * local, i1 = i0 + 1;
+    const bool has1 = i1 < H;
+    for (int k = threadIdx.x; k < W; k += T) {
+        const float a = G.T[(size_t)i0 * P + k];
+        const float b = has1 ? G.T[(size_t)i1 * P + k] : 0.f;
+        sm[k] = make_float2(a, b);
+    }
+    __syncthreads();
+    const float2* __restrict__ dw = G.prow.dctw;
+    for (int k = threadIdx.x; k <= W / 2; k += T) {
+        const int km = k == 0 ? 0 : W - k;
+        if (k > km) continue;
+        const float2 Yk = sm[k], Ym = sm[km];
+        const float2 wk = __ldg(&dw[k]);
+        const float mak = k == 0 ? 0.f : Ym.x, mbk = k == 0 ? 0.f : Ym.y;
+        const float2 Pak = cmul(cconj(wk), make_float2(Yk.x, -mak));
+        const float2 Pbk = cmul(cconj(wk), make_float2(Yk.y, -mbk));
+        const float2 Ck = cconj(make_float2(Pak.x - Pbk.y, Pak.y + Pbk.x));
+        if (km != k) {
+            const float2 wm = __ldg(&dw[km]);
+            const float2 Pam = cmul(cconj(wm), make_float2(Ym.x, -Yk.x));
+            const float2 Pbm = cmul(cconj(wm), make_float2(Ym.y, -Yk.y));
+            sm[km] = cconj(make_float2(Pam.x - Pbm.y, Pam.y + Pbm.x));
+        }
+        sm[k] = Ck;
+    }
+    __syncthreads();
+    dft_n<T, EMAX>(sm, 1, G.prow);
+    double acc[2] = {0.0, 0.0};
+    for (int j = threadIdx.x; j < W; j += T) {
+        const float2 v = sm[mk_perm(j, W)];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            if (h == 1 && !has1) break;
+            const int i = i0 + h;
+            const size_t o = (size_t)i * P + j;
+            const float zv = h == 0 ? v.x : -v.y;
+            if (MODE == 3) {
+                G.z[o] = zv;
+            } else if (MODE == 0) {
+                const float u = isfinite(zv) ? zv : 0.f;
+                acc[1] += isfinite(zv) ? 0.0 : 1.0;
+                G.U0[o] = u;
+                // (u * valid_float).sum(): an invalid pixel contributes u * 0
+                acc[0] += (double)(u * (G.valid[o] ? 1.f : 0.f));
+            } else {
+                G.z[o] = zv;
+                acc[0] += (double)G.r[o] * (double)zv;
+            }
+        }
+    }
+    if (MODE == 3) return;
+    if (arrive<2>(G, local, nct, acc, red)) {
+        finish_sum<2>(G, nct, acc, red);
+        if (threadIdx.x == 0) {
+            if (MODE == 0) {
+                if (acc[1] != 0.0) st->status |= 1;  // UNW_S_DCT_INIT_NONFINITE
+                st->mean = st->vcount > 0 ? acc[0] / st->vcount : 0.0;
+            } else if (MODE == 1) {
+                st->rz = acc[0];
+            } else {
+                const double rzn = acc[0];
+                if (fabs(st->rz) < 1e-15) {
+                    st->cg_active = 0;
+                } else {
+                    double be = rzn / st->rz;
+                    be = be < -1e6 ? -1e6 : (be > 1e6 ? 1e6 : be);
+                    st->beta = (float)be;
+                    st->rz = rzn;
+                }
+            }
+        }
+    }
+}
+
+// ============================================================ stencil kernels
+// KS_STEN shape: a CTA covers 256 columns x sten_rows rows.
+// matvec: p = z + beta p_old (p = z on the first PCG iteration), Ap = A p,
+// pAp = p.Ap (utils_unwrap2d.py:1430-1443, :1471).
+__device__ __forceinline__ float pnew_at(const float* __restrict__ z, const float* __restrict__ po,
+                                         size_t o, bool first, float beta) {
+    return first ? z[o] : fadd(fmul(po[o], beta), z[o]);
+}
+
+__global__ void __launch_bounds__(256) k_matvec(const GridDev* __restrict__ grids,
+                                                const int* __restrict__ starts, int n, int k) {
+    __shared__ double red[32 * 1];
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    InstState* st = G.st;
+    if (!(st->irls_active && st->cg_active)) return;
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int H = G.H, W = G.W, P = G.P;
+    const int tx = local % G.sten_tiles_x, ty = local / G.sten_tiles_x;
+    const int j = tx * 256 + threadIdx.x;
+    const int ib = ty * G.sten_rows, ie = min(H, ib + G.sten_rows);
+    const bool first = st->pfirst != 0;
+    const float beta = st->beta;
+    const float* __restrict__ z = G.z;
+    const float* __restrict__ po = (k & 1) ? G.p0 : G.p1;
+    float* __restrict__ pn = (k & 1) ? G.p1 : G.p0;
+    double acc[1] = {0.0};
+    if (j < W) {
+        for (int i = ib; i < ie; i++) {
+            const size_t o = (size_t)i * P + j;
+            const float pc = pnew_at(z, po, o, first, beta);
+            float res = 0.f;
+            if (j > 0) res = fsub(res, fmul(fsub(pc, pnew_at(z, po, o - 1, first, beta)), G.wIx[o - 1]));
+            if (j < W - 1) res = fadd(res, fmul(fsub(pnew_at(z, po, o + 1, first, beta), pc), G.wIx[o]));
+            if (i > 0) res = fsub(res, fmul(fsub(pc, pnew_at(z, po, o - P, first, beta)), G.wIy[o - P]));
+            if (i < H - 1) res = fadd(res, fmul(fsub(pnew_at(z, po, o + P, first, beta), pc), G.wIy[o]));
+            const float ap = -res;
+            pn[o] = pc;
+            G.Ap[o] = ap;
+            acc[0] += (double)pc * (double)ap;
+        }
+    }
+    if (arrive<1>(G, local, nct, acc, red)) {
+        finish_sum<1>(G, nct, acc, red);
+        if (threadIdx.x == 0) {
+            const double pAp = acc[0];
+            st->pAp = pAp;
+            st->cg_iter += 1;
+            st->pfirst = 0;
+            if (fabs(pAp) < 1e-15 || !isfinite(pAp)) {
+                st->cg_active = 0;
+            } else {
+                double a = st->rz / pAp;
+                a = a < -1e6 ? -1e6 : (a > 1e6 ? 1e6 : a);
+                st->alpha = (float)a;
+            }
+        }
+    }
+}
+
+// IRLS head (utils_unwrap2d.py:1536-1581): recentre, residual gradients,
+// best-iterate test, IRLS weights and right-hand side.  Reads U_cur, writes
+// the recentred iterate to U_nxt (U_cur keeps u_prev for the convergence test).
+__global__ void __launch_bounds__(256) k_head(const GridDev* __restrict__ grids,
+                                              const int* __restrict__ starts, int n, int it) {
+    __shared__ double red[32 * 2];
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    InstState* st = G.st;
+    if (!st->irls_active) return;
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int H = G.H, W = G.W, P = G.P;
+    const int tx = local % G.sten_tiles_x, ty = local / G.sten_tiles_x;
+    const int j = tx * 256 + threadIdx.x;
+    const int ib = ty * G.sten_rows, ie = min(H, ib + G.sten_rows);
+    const float m = st->vcount > 0 ? (float)st->mean : 0.f;
+    const float eps2 = st->eps2;
+    const float* __restrict__ uc = (it & 1) ? G.U1 : G.U0;
+    float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
+    double acc[2] = {0.0, 0.0};
+    if (j < W) {
+        for (int i = ib; i < ie; i++) {
+            const size_t o = (size_t)i * P + j;
+            const float c = fsub(uc[o], m);
+            // residual gradients r = grad(u) - g (last column/row: 0 - g)
+            const float rx = (j < W - 1) ? fsub(fsub(fsub(uc[o + 1], m), c), G.gx[o]) : fsub(0.f, G.gx[o]);
+            const float ry = (i < H - 1) ? fsub(fsub(fsub(uc[o + P], m), c), G.gy[o]) : fsub(0.f, G.gy[o]);
+            acc[0] += (double)fmul(rx, rx) + (double)fmul(ry, ry);
+            acc[1] += isfinite(c) ? 0.0 : 1.0;
+            const float wix = clampf_nan(fdiv(G.wx[o], __fsqrt_rn(fadd(fmul(rx, rx), eps2))), 1e-6f, 1e6f);
+            const float wiy = clampf_nan(fdiv(G.wy[o], __fsqrt_rn(fadd(fmul(ry, ry), eps2))), 1e-6f, 1e6f);
+            float bv = 0.f;
+            if (j > 0) {
+                const float l = fsub(uc[o - 1], m);
+                const float rxl = fsub(fsub(c, l), G.gx[o - 1]);
+                const float wl = clampf_nan(fdiv(G.wx[o - 1], __fsqrt_rn(fadd(fmul(rxl, rxl), eps2))), 1e-6f, 1e6f);
+                bv = fadd(bv, fmul(wl, G.gx[o - 1]));
+            }
+            if (j < W - 1) bv = fsub(bv, fmul(wix, G.gx[o]));
+            if (i > 0) {
+                const float u = fsub(uc[o - P], m);
+                const float ryu = fsub(fsub(c, u), G.gy[o - P]);
+                const float wu = clampf_nan(fdiv(G.wy[o - P], __fsqrt_rn(fadd(fmul(ryu, ryu), eps2))), 1e-6f, 1e6f);
+                bv = fadd(bv, fmul(wu, G.gy[o - P]));
+            }
+            if (i < H - 1) bv = fsub(bv, fmul(wiy, G.gy[o]));
+            un[o] = c;
+            G.wIx[o] = wix;
+            G.wIy[o] = wiy;
+            G.b[o] = bv;
+        }
+    }
+    if (arrive<2>(G, local, nct, acc, red)) {
+        finish_sum<2>(G, nct, acc, red);
+        if (threadIdx.x == 0) {
+            const double res = acc[0];
+            st->residual = res;
+            st->best_update = 0;
+            if (res < st->best_residual && acc[1] == 0.0) {
+                st->best_residual = res;
+                st->best_update = 1;
+            }
+            st->cg_active = 1;
+            st->cg_iter = 0;
+            st->pfirst = 1;
+        }
+    }
+}
+
+// ============================================================ elementwise kernels (KS_ELEM)
+// sum over all pixels of u * valid (utils_unwrap2d.py:1539-1541)
+__global__ void k_mean(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n, int it) {
+    __shared__ double red[32 * 1];
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    InstState* st = G.st;
+    if (!st->irls_active) return;
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int W = G.W, P = G.P;
+    const long long npx = (long long)G.H * W;
+    const float* __restrict__ uc = (it & 1) ? G.U1 : G.U0;
+    double acc[1] = {0.0};
+    for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
+        const int i = (int)(q / W), j = (int)(q - (long long)i * W);
+        const size_t o = (size_t)i * P + j;
+        acc[0] += (double)(uc[o] * (G.valid[o] ? 1.f : 0.f));
+    }
+    if (arrive<1>(G, local, nct, acc, red)) {
+        finish_sum<1>(G, nct, acc, red);
+        if (threadIdx.x == 0) st->mean = st->vcount > 0 ? acc[0] / st->vcount : 0.0;
+    }
+}
+
+// After the DCT initial solve: u -= mean_valid(u); u_best = u (utils_unwrap2d.py:1509-1531).
+__global__ void k_init_recentre(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    const InstState* st = G.st;
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int W = G.W, P = G.P;
+    const long long npx = (long long)G.H * W;
+    const float m = st->vcount > 0 ? (float)st->mean : 0.f;
+    for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
+        const int i = (int)(q / W), j = (int)(q - (long long)i * W);
+        const size_t o = (size_t)i * P + j;
+        const float u = fsub(G.U0[o], m);
+        G.U0[o] = u;
+        G.Ub[o] = u;
+    }
+}
+
+// u_best = u_rc when the head found a smaller residual (utils_unwrap2d.py:1555-1558)
+__global__ void k_copy_best(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n, int it) {
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    const InstState* st = G.st;
+    if (!(st->irls_active && st->best_update)) return;
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int W = G.W, P = G.P;
+    const long long npx = (long long)G.H * W;
+    const float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
+    for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
+        const int i = (int)(q / W), j = (int)(q - (long long)i * W);
+        const size_t o = (size_t)i * P + j;
+        G.Ub[o] = un[o];
+    }
+}
+
+// IRLS tail (utils_unwrap2d.py:1599-1626): non-finite -> revert to u_best and
+// stop; rel_change = |u_prev - u| / (|u| + 1e-10) over the full grid.
+__global__ void k_rel(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n, int it) {
+    __shared__ double red[32 * 3];
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    InstState* st = G.st;
+    if (!st->irls_active) return;
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int W = G.W, P = G.P;
+    const long long npx = (long long)G.H * W;
+    const float* __restrict__ up = (it & 1) ? G.U1 : G.U0;
+    const float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
+        const int i = (int)(q / W), j = (int)(q - (long long)i * W);
+        const size_t o = (size_t)i * P + j;
+        const float u = un[o];
+        const float d = fsub(up[o], u);
+        acc[0] += (double)d * (double)d;
+        acc[1] += (double)u * (double)u;
+        acc[2] += isfinite(u) ? 0.0 : 1.0;
+    }
+    if (arrive<3>(G, local, nct, acc, red)) {
+        finish_sum<3>(G, nct, acc, red);
+        if (threadIdx.x == 0) {
+            const int t = st->irls_iter;
+            if (t < UNW_MAX_LOG) st->cg_log[t] = st->cg_iter;
+            st->cg_total += st->cg_iter;
+            st->irls_iter = t + 1;
+            if (acc[2] != 0.0) {
+                st->u_index = 2;             // u_best holds the result
+                st->status |= 2;             // UNW_S_REVERTED
+                st->irls_active = 0;
+            } else {
+                st->u_index = (it & 1) ? 0 : 1;
+                const double rel = sqrt(acc[0]) / (sqrt(acc[1]) + 1e-10);
+                st->rel_change = rel;
+                if (rel < (double)st->tol || st->irls_iter >= st->max_iter) st->irls_active = 0;
+            }
+        }
+    }
+}
+
+// Ax for a whole grid (operator entry point unw_apply_laplacian), x = G.r, Ax -> G.Ap.
+__global__ void k_lap_apply(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int H = G.H, W = G.W, P = G.P;
+    const long long npx = (long long)H * W;
+    for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
+        const int i = (int)(q / W), j = (int)(q - (long long)i * W);
+        G.Ap[(size_t)i * P + j] = lap_at(G.r, G.wIx, G.wIy, i, j, H, W, P);
+    }
+}
+
+// ============================================================ launchers
+template <int MODE>
+static cudaError_t launch_row_fwd_t(int T, int emax, dim3 grid, size_t smem, cudaStream_t s,
+                                    const GridDev* gd, const int* st, int n, int it, int cgk) {
+#define UNW_RF(TT, EE)                                                                      \
+    if (T == TT && emax == EE) {                                                            \
+        auto kfn = k_row_fwd<TT, EE, MODE>;                                                 \
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+        kfn<<<grid, TT, smem, s>>>(gd, st, n, it, cgk);                                     \
+        return cudaGetLastError();                                                          \
+    }
+    UNW_RF(128, 16) UNW_RF(256, 16) UNW_RF(512, 16) UNW_RF(1024, 16)
+#undef UNW_RF
+    return cudaErrorInvalidConfiguration;
+}
+
+cudaError_t unw_launch_row_fwd(int mode, int T, int emax, int nblk, size_t smem, cudaStream_t s,
+                               const GridDev* gd, const int* starts, int n, int it, int cgk) {
+    if (nblk <= 0) return cudaSuccess;
+    dim3 grid(nblk);
+    switch (mode) {
+        case 0: return launch_row_fwd_t<0>(T, emax, grid, smem, s, gd, starts, n, it, cgk);
+        case 1: return launch_row_fwd_t<1>(T, emax, grid, smem, s, gd, starts, n, it, cgk);
+        case 2: return launch_row_fwd_t<2>(T, emax, grid, smem, s, gd, starts, n, it, cgk);
+        default: return launch_row_fwd_t<3>(T, emax, grid, smem, s, gd, starts, n, it, cgk);
+    }
+}
+
+template <int MODE>
+static cudaError_t launch_row_inv_t(int T, int emax, dim3 grid, size_t smem, cudaStream_t s,
+                                    const GridDev* gd, const int* st, int n) {
+#define UNW_RI(TT, EE)                                                                      \
+    if (T == TT && emax == EE) {                                                            \
+        auto kfn = k_row_inv<TT, EE, MODE>;                                                 \
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+        kfn<<<grid, TT, smem, s>>>(gd, st, n);                                              \
+        return cudaGetLastError();                                                          \
+    }
+    UNW_RI(128, 16) UNW_RI(256, 16) UNW_RI(512, 16) UNW_RI(1024, 16)
+#undef UNW_RI
+    return cudaErrorInvalidConfiguration;
+}
+
+cudaError_t unw_launch_row_inv(int mode, int T, int emax, int nblk, size_t smem, cudaStream_t s,
+                               const GridDev* gd, const int* starts, int n) {
+    if (nblk <= 0) return cudaSuccess;
+    dim3 grid(nblk);
+    switch (mode) {
+        case 0: return launch_row_inv_t<0>(T, emax, grid, smem, s, gd, starts, n);
+        case 1: return launch_row_inv_t<1>(T, emax, grid, smem, s, gd, starts, n);
+        case 2: return launch_row_inv_t<2>(T, emax, grid, smem, s, gd, starts, n);
+        default: return launch_row_inv_t<3>(T, emax, grid, smem, s, gd, starts, n);
+    }
+}
+
+template <int MODE>
+static cudaError_t launch_col_t(int T, int emax, dim3 grid, size_t smem, cudaStream_t s,
+                                const GridDev* gd, const int* st, int n) {
+#define UNW_CL(TT, EE)                                                                      \
+    if (T == TT && emax == EE) {                                                            \
+        auto kfn = k_col<TT, EE, MODE>;                                                     \
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+        kfn<<<grid, TT, smem, s>>>(gd, st, n);                                              \
+        return cudaGetLastError();                                                          \
+    }
+    UNW_CL(128, 16) UNW_CL(256, 16) UNW_CL(512, 16) UNW_CL(1024, 16)
+#undef UNW_CL
+    return cudaErrorInvalidConfiguration;
+}
+
+cudaError_t unw_launch_col(int mode, int T, int emax, int nblk, size_t smem, cudaStream_t s,
+                           const GridDev* gd, const int* starts, int n) {
+    if (nblk <= 0) return cudaSuccess;
+    dim3 grid(nblk);
+    return mode == 0 ? launch_col_t<0>(T, emax, grid, smem, s, gd, starts, n)
+                     : launch_col_t<1>(T, emax, grid, smem, s, gd, starts, n);
+}
+
+cudaError_t unw_launch_tables(const FftPlanDev& f, const DctPlanDev& d, double* cosv, int Ncos,
+                              cudaStream_t s) {
+    int m = f.n > d.N ? f.n : d.N;
+    m = m > Ncos ? m : Ncos;
+    int nb = (m + 255) / 256;
+    nb = nb > 64 ? 64 : nb;
+    k_tables<<<nb, 256, 0, s>>>(f, d, cosv, Ncos);
+    return cudaGetLastError();
+}
+
+cudaError_t unw_launch_hspec(int T, int emax, const DctPlanDev& d, cudaStream_t s) {
+    const size_t smem = (size_t)d.fft.n * sizeof(float2);
+#define UNW_HS(TT, EE)                                                                      \
+    if (T == TT && emax == EE) {                                                            \
+        auto kfn = k_hspec<TT, EE>;                                                         \
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+        kfn<<<1, TT, smem, s>>>(d);                                                         \
+        return cudaGetLastError();                                                          \
+    }
+    UNW_HS(128, 16) UNW_HS(256, 16) UNW_HS(512, 16) UNW_HS(1024, 16)
+#undef UNW_HS
+    return cudaErrorInvalidConfiguration;
+}
+
+cudaError_t unw_launch_simple(int which, int nblk, cudaStream_t s, const GridDev* gd,
+                              const int* starts, int n, int it, UnwScalars sc) {
+    if (nblk <= 0) return cudaSuccess;
+    switch (which) {
+        case UNW_K_STATE_INIT: k_state_init<<<(n + 63) / 64, 64, 0, s>>>(gd, n, sc); break;
+        case UNW_K_SETUP: k_setup<<<nblk, 256, 0, s>>>(gd, starts, n); break;
+        case UNW_K_MATVEC: k_matvec<<<nblk, 256, 0, s>>>(gd, starts, n, it); break;
+        case UNW_K_HEAD: k_head<<<nblk, 256, 0, s>>>(gd, starts, n, it); break;
+        case UNW_K_MEAN: k_mean<<<nblk, 256, 0, s>>>(gd, starts, n, it); break;
+        case UNW_K_INIT_RECENTRE: k_init_recentre<<<nblk, 256, 0, s>>>(gd, starts, n); break;
+        case UNW_K_COPY_BEST: k_copy_best<<<nblk, 256, 0, s>>>(gd, starts, n, it); break;
+        case UNW_K_REL: k_rel<<<nblk, 256, 0, s>>>(gd, starts, n, it); break;
+        case UNW_K_LAP_APPLY: k_lap_apply<<<nblk, 256, 0, s>>>(gd, starts, n); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}

@@ -1,0 +1,240 @@
+"""Drop-in replacement for insardev's `irls_unwrap_2d` on NVIDIA B200 GPUs.
+
+`irls_unwrap_2d` keeps the reference signature, argument meaning, output
+conventions and error behaviour of insardev/insardev/utils_unwrap2d.py:1082:
+
+* `phase` 2-D float array (NaN = invalid), numpy or torch (CPU or CUDA);
+  non-contiguous views are accepted;
+* `weight` same shape or None (NaN allowed; clipped to [0.01, 1] after NaN
+  zeroing, like :1233-1238);
+* returns `(unwrapped float32 [H,W] with NaN where invalid,
+  conncomp uint16 [H,W], 0 = invalid/small, 1 = largest, ...)`, numpy arrays
+  for numpy input, torch tensors on the device for CUDA tensor input;
+* `ValueError` for non-2-D input; all-NaN input -> (NaN, zeros); a
+  non-finite solution -> `RuntimeWarning` and (NaN, zeros).
+
+The solve runs entirely in libunwrap_b200.so (hand-written sm_100a kernels);
+PyTorch only provides device memory and the stream.  Devices other than CUDA
+are rejected: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+import warnings
+
+import numpy as np
+
+from . import _lib
+
+FN_DEFAULTS = dict(max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2, conncomp_size=30)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def resolve_device(device, phase=None):
+    """'auto' / 'cuda' / 'cuda:N' / torch.device -> a CUDA torch.device (else raise)."""
+    torch = _torch()
+    if isinstance(phase, torch.Tensor) and phase.is_cuda and device in ("auto", None):
+        return phase.device
+    if device in ("auto", None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("core_b200.irls_unwrap_2d needs a CUDA GPU; none is visible")
+        return torch.device("cuda", torch.cuda.current_device())
+    dev = torch.device(device) if not isinstance(device, torch.device) else device
+    if dev.type != "cuda":
+        raise ValueError(f"core_b200.irls_unwrap_2d runs on CUDA devices only, got device={device!r}")
+    if dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    return dev
+
+
+def make_params(max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2, conncomp_size=30,
+                congruent=False, check_every=1):
+    p = _lib.UnwParams()
+    p.max_iter = int(max_iter)
+    p.tol = float(tol)
+    p.cg_max_iter = int(cg_max_iter)
+    p.cg_tol = float(cg_tol)
+    p.epsilon = float(epsilon)
+    p.conncomp_size = int(conncomp_size)
+    p.flags = _lib.UNW_F_CONGRUENT if congruent else 0
+    p.check_every = int(check_every)
+    return p
+
+
+def _to_device_f32(a, dev):
+    """Contiguous float32 CUDA tensor from numpy / torch input (copies only when needed)."""
+    torch = _torch()
+    if isinstance(a, torch.Tensor):
+        t = a.to(device=dev, dtype=torch.float32, non_blocking=a.device.type == "cpu" and a.is_pinned())
+        return t.contiguous()
+    arr = np.ascontiguousarray(a, dtype=np.float32)
+    return torch.from_numpy(arr).to(dev)
+
+
+class _Workspace:
+    """Per-device workspace cache (the caching allocator would also reuse it)."""
+
+    def __init__(self):
+        self.buf = {}
+
+    def get(self, dev, nbytes):
+        torch = _torch()
+        key = (dev.type, dev.index)
+        b = self.buf.get(key)
+        if b is None or b.numel() < nbytes:
+            self.buf.pop(key, None)
+            b = torch.empty(int(nbytes), dtype=torch.uint8, device=dev)
+            self.buf[key] = b
+        return b
+
+
+_WS_LOCAL = threading.local()
+
+
+def _ws():
+    if not hasattr(_WS_LOCAL, "ws"):
+        _WS_LOCAL.ws = _Workspace()
+    return _WS_LOCAL.ws
+
+
+def irls_unwrap_2d(phase, weight=None, device='auto', max_iter=50, tol=1e-3,
+                   cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2, conncomp_size=30, debug=False,
+                   *, congruent=False, return_stats=False, check_every=1):
+    """Unwrap 2-D phase with the DCT-preconditioned IRLS L1 solver on a B200.
+
+    Same parameters and outputs as the reference (utils_unwrap2d.py:1082-1083).
+    Keyword-only extras (defaults keep the reference behaviour):
+      congruent     return phase + 2*pi*round((u - phase)/2pi) instead of u
+      return_stats  also return a dict of iteration counts and status bits
+      check_every   IRLS iterations enqueued between device->host convergence reads
+    """
+    torch = _torch()
+    is_torch = isinstance(phase, torch.Tensor)
+    if phase.ndim != 2:
+        raise ValueError(f"irls_unwrap_2d expects 2D phase array, got shape {tuple(phase.shape)}")
+    dev = resolve_device(device, phase)
+    lib = _lib.load()
+    H, W = int(phase.shape[0]), int(phase.shape[1])
+    with torch.cuda.device(dev):
+        ph = _to_device_f32(phase, dev)
+        wt = _to_device_f32(weight, dev) if weight is not None else None
+        if wt is not None and tuple(wt.shape) != (H, W):
+            raise ValueError(f"weight shape {tuple(wt.shape)} differs from phase shape {(H, W)}")
+        out_u = torch.empty((H, W), dtype=torch.float32, device=dev)
+        out_cc = torch.empty((H, W), dtype=torch.int16, device=dev)
+        nbytes = lib.unw_workspace_bytes(H, W)
+        ws = _ws().get(dev, nbytes)
+        st = _lib.UnwStats()
+        prm = make_params(max_iter, tol, cg_max_iter, cg_tol, epsilon, conncomp_size, congruent, check_every)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        rc = lib.unw_solve_f32(ph.data_ptr(), W, wt.data_ptr() if wt is not None else None, W, H, W,
+                               C.byref(prm), out_u.data_ptr(), W, out_cc.data_ptr(), W,
+                               ws.data_ptr(), ws.numel(), C.byref(st), stream)
+        _lib.check(rc, "unw_solve_f32")
+    stats = st.as_dict()
+    if debug:
+        _print_debug(H, W, stats)
+    if st.status & _lib.UNW_S_ALL_NAN:
+        # utils_unwrap2d.py:1200-1201 returns full_like(phase, nan) in the input dtype
+        if is_torch:
+            res = (torch.full_like(phase, float("nan")), torch.zeros((H, W), dtype=torch.int16, device=phase.device))
+        else:
+            res = (np.full_like(phase, np.nan), np.zeros((H, W), dtype=np.uint16))
+        return res + (stats,) if return_stats else res
+    if rc == _lib.UNW_W_NUMERIC:
+        warnings.warn("IRLS produced NaN/inf values - returning NaN for this component", RuntimeWarning)
+    if is_torch and phase.is_cuda:
+        res = (out_u, out_cc.view(torch.uint16) if hasattr(torch, "uint16") else out_cc)
+    else:
+        res = (out_u.cpu().numpy(), out_cc.cpu().numpy().view(np.uint16))
+    return res + (stats,) if return_stats else res
+
+
+def irls_unwrap_2d_batch(phases, weights=None, device='auto', max_iter=50, tol=1e-3, cg_max_iter=20,
+                         cg_tol=1e-4, epsilon=1e-2, conncomp_size=30, debug=False, *, congruent=False,
+                         return_stats=False, check_every=1):
+    """Unwrap a list of independent grids (any sizes) in one batched launch sequence.
+
+    Each grid converges on its own test, exactly as if `irls_unwrap_2d` had been
+    called on it alone.  Returns a list of (unwrapped, conncomp) tuples.
+    """
+    torch = _torch()
+    phases = list(phases)
+    n = len(phases)
+    if n == 0:
+        return []
+    weights = [None] * n if weights is None else list(weights)
+    if len(weights) != n:
+        raise ValueError("weights must match phases")
+    for p in phases:
+        if p.ndim != 2:
+            raise ValueError(f"irls_unwrap_2d expects 2D phase array, got shape {tuple(p.shape)}")
+    dev = resolve_device(device, phases[0])
+    lib = _lib.load()
+    grids = (_lib.UnwGrid * n)()
+    keep = []
+    outs = []
+    Hs = (C.c_int64 * n)()
+    Ws = (C.c_int64 * n)()
+    with torch.cuda.device(dev):
+        for g, (p, w) in enumerate(zip(phases, weights)):
+            H, W = int(p.shape[0]), int(p.shape[1])
+            ph = _to_device_f32(p, dev)
+            wt = _to_device_f32(w, dev) if w is not None else None
+            ou = torch.empty((H, W), dtype=torch.float32, device=dev)
+            oc = torch.empty((H, W), dtype=torch.int16, device=dev)
+            keep += [ph, wt]
+            outs.append((ou, oc))
+            grids[g].phase = ph.data_ptr()
+            grids[g].phase_pitch = W
+            grids[g].weight = wt.data_ptr() if wt is not None else None
+            grids[g].weight_pitch = W
+            grids[g].H = H
+            grids[g].W = W
+            grids[g].out_u = ou.data_ptr()
+            grids[g].out_u_pitch = W
+            grids[g].out_cc = oc.data_ptr()
+            grids[g].out_cc_pitch = W
+            Hs[g] = H
+            Ws[g] = W
+        nbytes = lib.unw_batch_workspace_bytes(n, Hs, Ws)
+        ws = _ws().get(dev, nbytes)
+        sts = (_lib.UnwStats * n)()
+        prm = make_params(max_iter, tol, cg_max_iter, cg_tol, epsilon, conncomp_size, congruent, check_every)
+        rc = lib.unw_solve_batch(n, grids, C.byref(prm), ws.data_ptr(), ws.numel(), sts,
+                                 torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(rc, "unw_solve_batch")
+    res = []
+    for g in range(n):
+        st = sts[g]
+        p = phases[g]
+        is_torch = isinstance(p, torch.Tensor)
+        ou, oc = outs[g]
+        if debug:
+            _print_debug(int(p.shape[0]), int(p.shape[1]), st.as_dict())
+        if st.status & _lib.UNW_S_ALL_NAN:
+            r = ((torch.full_like(p, float("nan")), torch.zeros_like(oc)) if is_torch
+                 else (np.full_like(p, np.nan), np.zeros(p.shape, dtype=np.uint16)))
+        else:
+            if st.status & _lib.UNW_S_NONFINITE_OUT:
+                warnings.warn("IRLS produced NaN/inf values - returning NaN for this component", RuntimeWarning)
+            r = ((ou, oc.view(torch.uint16) if hasattr(torch, "uint16") else oc) if is_torch and p.is_cuda
+                 else (ou.cpu().numpy(), oc.cpu().numpy().view(np.uint16)))
+        res.append(r + (st.as_dict(),) if return_stats else r)
+    return res
+
+
+def _print_debug(H, W, s):
+    r0, r1, c0, c1 = s["bbox"]
+    print(f"  Cropped to bbox [{r0}:{r1}, {c0}:{c1}] = {r1 - r0}x{c1 - c0} (from {H}x{W})")
+    for i, cg in enumerate(s["cg_iters"]):
+        if i % 5 == 0:
+            print(f"  IRLS iter {i}: cg_iters = {cg}")
+    print(f"  IRLS iters: {s['irls_iters']} iterations, rel_change = {s['rel_change']:.2e}, "
+          f"best residual = {s['best_residual']:.3e}")
+    print(f"  conncomp: {s['n_components']} kept of {s['n_labels']}")

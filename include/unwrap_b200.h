@@ -1,0 +1,150 @@
+/*
+ * unwrap_b200.h — C ABI of the B200 (sm_100a) DCT+IRLS L1 2-D phase unwrapper.
+ *
+ * Drop-in boundary for insardev's `irls_unwrap_2d`
+ * (insardev/insardev/utils_unwrap2d.py:1082-1766).  All pointers are device
+ * pointers unless stated; all calls are thread safe (every piece of mutable
+ * state lives in the caller's workspace) and run on the caller's CUDA stream.
+ * Calls that must read a device scalar to decide what to do next (bounding
+ * box, IRLS convergence, component count) synchronise that stream.
+ *
+ * Return codes: 0 ok; negative = error (see UNW_E_*), message via
+ * unw_last_error().  UNW_W_NUMERIC (>0) is the reference's "NaN/inf produced"
+ * outcome (utils_unwrap2d.py:1659-1665): outputs are all-NaN / all-zero and a
+ * caller mirroring the reference raises RuntimeWarning.
+ */
+#ifndef UNWRAP_B200_H
+#define UNWRAP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define UNW_API __attribute__((visibility("default")))
+#else
+#define UNW_API
+#endif
+
+#define UNW_ABI_VERSION 1
+
+enum {
+    UNW_OK = 0,
+    UNW_W_NUMERIC = 1,      /* non-finite solution on valid pixels: NaN output  */
+    UNW_E_ARG = -1,         /* bad argument (null pointer, shape, pitch)        */
+    UNW_E_WORKSPACE = -2,   /* workspace too small                              */
+    UNW_E_CUDA = -3,        /* CUDA runtime error                               */
+    UNW_E_UNSUPPORTED = -4, /* grid dimension beyond the transform limits       */
+    UNW_E_OVERFLOW = -5     /* > 65535 kept components (uint16 labels)           */
+};
+
+/* Solver parameters: same names and meaning as the reference keywords
+ * (utils_unwrap2d.py:1082-1083).  `flags` holds UNW_F_* bits. */
+typedef struct unw_params {
+    int32_t max_iter;       /* IRLS iterations (reference default 50)          */
+    float tol;              /* IRLS relative-change tolerance (1e-3)           */
+    int32_t cg_max_iter;    /* PCG iterations per IRLS step (20)               */
+    float cg_tol;           /* absolute PCG residual-norm tolerance (1e-4)     */
+    float epsilon;          /* L1 smoothing (1e-2)                             */
+    int32_t conncomp_size;  /* minimum kept component size (30)                */
+    int32_t flags;
+    int32_t check_every;    /* IRLS iterations enqueued between host checks    */
+} unw_params;
+
+#define UNW_F_CONGRUENT 1   /* output phase + 2*pi*k instead of the smooth solution */
+#define UNW_F_NO_GRAPH  2   /* launch kernels one by one instead of a CUDA graph    */
+
+/* Per-solve statistics (the reference prints these under debug=True). */
+typedef struct unw_stats {
+    int32_t irls_iters;     /* IRLS iterations run                              */
+    int32_t cg_iters_total; /* PCG iterations summed over IRLS iterations        */
+    int32_t cg_iters_last;  /* PCG iterations of the last IRLS iteration         */
+    int32_t n_components;   /* kept components (labels 1..n)                    */
+    int32_t n_labels;       /* 4-connected components before the size filter    */
+    int32_t status;         /* UNW_S_* bits                                     */
+    int32_t bbox[4];        /* r0, r1, c0, c1 of the valid bounding box          */
+    double rel_change;      /* last IRLS relative change                         */
+    double best_residual;   /* best sum of squared gradient residuals            */
+    double k_median;        /* median 2-pi cycle shift applied                   */
+    int32_t cg_iters[64];   /* PCG iterations of the first 64 IRLS iterations    */
+} unw_stats;
+
+#define UNW_S_DCT_INIT_NONFINITE 1   /* DCT init produced NaN/inf (zero-filled)  */
+#define UNW_S_REVERTED           2   /* reverted to the best iterate             */
+#define UNW_S_NONFINITE_OUT      4   /* non-finite output: NaN result            */
+#define UNW_S_ALL_NAN            8   /* input all NaN                            */
+
+/* One grid of a batched solve (unw_solve_batch).  Pitches are in elements. */
+typedef struct unw_grid {
+    const float* phase;     int64_t phase_pitch;
+    const float* weight;    int64_t weight_pitch;   /* NULL = uniform weights   */
+    int64_t H, W;
+    float* out_u;           int64_t out_u_pitch;
+    uint16_t* out_cc;       int64_t out_cc_pitch;
+} unw_grid;
+
+UNW_API int unw_abi_version(void);
+
+/* Thread-local text of the last error on this thread. */
+UNW_API const char* unw_last_error(void);
+
+/* Device workspace bytes needed to solve one H x W grid. */
+UNW_API size_t unw_workspace_bytes(int64_t H, int64_t W);
+
+/* Device workspace bytes for a batch of n grids solved together. */
+UNW_API size_t unw_batch_workspace_bytes(int32_t n, const int64_t* H, const int64_t* W);
+
+/*
+ * Unwrap one grid.  Replaces utils_unwrap2d.py:1082 irls_unwrap_2d.
+ *   phase  [H][phase_pitch]  float32, NaN = invalid (device)
+ *   weight [H][weight_pitch] float32 or NULL (device)
+ *   out_u  [H][out_u_pitch]  float32 (device): unwrapped phase, NaN where invalid
+ *   out_cc [H][out_cc_pitch] uint16  (device): 0 invalid/small, 1 largest, ...
+ *   stats  host pointer or NULL.
+ */
+UNW_API int unw_solve_f32(const float* phase, int64_t phase_pitch,
+                  const float* weight, int64_t weight_pitch,
+                  int64_t H, int64_t W, const unw_params* params,
+                  float* out_u, int64_t out_u_pitch,
+                  uint16_t* out_cc, int64_t out_cc_pitch,
+                  void* workspace, size_t workspace_bytes,
+                  unw_stats* stats, void* cuda_stream);
+
+/*
+ * Unwrap n independent grids of any sizes in one launch sequence: every kernel
+ * covers all still-active grids, each grid stops on its own convergence test.
+ * Replaces the per-pair loop of Stack_unwrap2d.py:102-130 (_irls_overlap_kernel)
+ * and the per-task calls of Stack_unwrap2d.py:32-71.  stats: n entries or NULL.
+ */
+UNW_API int unw_solve_batch(int32_t n, const unw_grid* grids, const unw_params* params,
+                    void* workspace, size_t workspace_bytes,
+                    unw_stats* stats, void* cuda_stream);
+
+/*
+ * Operator entry points (one H x W grid, dense pitch = W, device pointers).
+ * They expose single steps of the solver for verification.
+ */
+
+/* Wrapped gradients and edge weights, utils_unwrap2d.py:1228-1275.
+ * Outputs gx, gy, wx, wy: [H][W] float32; valid: [H][W] uint8. */
+UNW_API int unw_setup_gradients(const float* phase, const float* weight, int64_t H, int64_t W,
+                        float* gx, float* gy, float* wx, float* wy, uint8_t* valid,
+                        void* workspace, size_t workspace_bytes, void* cuda_stream);
+
+/* Weighted-Laplacian matvec Ax = -div(w grad x), utils_unwrap2d.py:1367-1388. */
+UNW_API int unw_apply_laplacian(const float* x, const float* wx, const float* wy,
+                        int64_t H, int64_t W, float* Ax,
+                        void* workspace, size_t workspace_bytes, void* cuda_stream);
+
+/* DCT preconditioner z = IDCT2(-DCT2(r)/lambda), DC term zeroed,
+ * utils_unwrap2d.py:1390-1403 (also the DCT initial solve :1478-1513). */
+UNW_API int unw_apply_preconditioner(const float* r, int64_t H, int64_t W, float* z,
+                             void* workspace, size_t workspace_bytes, void* cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UNWRAP_B200_H */

@@ -1,0 +1,76 @@
+"""C ABI: the library loads without a GPU, exports every symbol the header
+declares, sizes workspaces, and rejects bad arguments before any CUDA call."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+from core_b200 import _lib
+
+HEADER = os.path.join(REPO, "include", "unwrap_b200.h")
+
+
+def header_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"UNW_API\s+[\w\s\*]+?\b(unw_\w+)\s*\(", txt)))
+
+
+def test_header_declares_expected_entry_points():
+    syms = header_symbols()
+    for s in ("unw_solve_f32", "unw_solve_batch", "unw_workspace_bytes", "unw_last_error",
+              "unw_apply_laplacian", "unw_apply_preconditioner", "unw_setup_gradients"):
+        assert s in syms
+
+
+def test_library_exports_every_header_symbol():
+    lib = _lib.load()
+    for s in header_symbols():
+        assert hasattr(lib, s), s
+        assert s in _lib.SIGNATURES, s
+    assert lib.unw_abi_version() == 1
+
+
+def test_workspace_bytes_monotone_and_sane():
+    lib = _lib.load()
+    a = lib.unw_workspace_bytes(1024, 1024)
+    b = lib.unw_workspace_bytes(4096, 4096)
+    assert 0 < a < b
+    # about 16 float arrays + masks per pixel, well under 100 B/px
+    assert 60 * 4096 * 4096 < b < 100 * 4096 * 4096
+    assert lib.unw_workspace_bytes(0, 5) == 0
+    H = (C.c_int64 * 2)(100, 200)
+    W = (C.c_int64 * 2)(300, 50)
+    both = lib.unw_batch_workspace_bytes(2, H, W)
+    assert both >= lib.unw_workspace_bytes(100, 300) + lib.unw_workspace_bytes(200, 50) - 4096
+
+
+def test_solve_rejects_bad_args_without_gpu():
+    lib = _lib.load()
+    prm = _lib.UnwParams(50, 1e-3, 20, 1e-4, 1e-2, 30, 0, 1)
+    fake = C.c_void_p(0x10000)
+    rc = lib.unw_solve_f32(None, 8, None, 8, 8, 8, C.byref(prm), fake, 8, fake, 8, fake, 1 << 30, None, None)
+    assert rc == _lib.UNW_E_ARG and "null" in _lib.last_error()
+    rc = lib.unw_solve_f32(fake, 4, None, 8, 8, 8, C.byref(prm), fake, 8, fake, 8, fake, 1 << 30, None, None)
+    assert rc == _lib.UNW_E_ARG and "pitch" in _lib.last_error()
+    rc = lib.unw_solve_f32(fake, 8, None, 8, 8, 8, C.byref(prm), fake, 8, fake, 8, fake, 16, None, None)
+    assert rc == _lib.UNW_E_WORKSPACE
+    bad = _lib.UnwParams(-1, 1e-3, 20, 1e-4, 1e-2, 30, 0, 1)
+    rc = lib.unw_solve_f32(fake, 8, None, 8, 8, 8, C.byref(bad), fake, 8, fake, 8, fake, 1 << 30, None, None)
+    assert rc == _lib.UNW_E_ARG
+    with pytest.raises(ValueError):
+        _lib.check(_lib.UNW_E_ARG)
+    with pytest.raises(OverflowError):
+        _lib.check(_lib.UNW_E_OVERFLOW)
+
+
+def test_python_boundary_validation_without_gpu():
+    import core_b200
+    with pytest.raises(ValueError):
+        core_b200.irls_unwrap_2d(np.zeros((2, 3, 4), np.float32))
+    with pytest.raises(ValueError):
+        core_b200.irls_unwrap_2d(np.zeros((4, 4), np.float32), device="cpu")
+    with pytest.raises(ValueError):
+        core_b200.irls_unwrap_2d(np.zeros((4, 4), np.float32), device="mps")

@@ -1,0 +1,313 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle and the
+reference's own outputs (tests/golden, made by running insardev's function).
+
+Tolerances (float32 solver, float64 reductions):
+  * operator kernels: matvec bit-exact to the reference's float32 op order
+    (checked <= 1e-6 relative); wrapped gradients <= 2e-6 rad (libm ulps);
+    DCT preconditioner <= 2e-5 relative to the float64 operator;
+  * full solves: NaN positions identical, 2-pi cycle map identical on
+    >= 99.99% of valid pixels, RMS difference after mean removal <= 1e-3 rad
+    against the reference's FP64 run (and its FP32 run), conncomp identical
+    (labels of equal-size components may be permuted; the reference leaves
+    that order to numpy's sort).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+import scipy.fft as sfft
+
+from conftest import load_golden, small_golden_names
+from oracle.generators import gen_g1, gen_g2
+from oracle.irls_oracle import cycle_map, irls_unwrap_2d as oracle_unwrap
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+import core_b200  # noqa: E402
+from core_b200 import _lib  # noqa: E402
+
+DEV = torch.device("cuda", 0)
+
+
+def _ws(H, W):
+    n = _lib.load().unw_workspace_bytes(H, W)
+    return torch.empty(n, dtype=torch.uint8, device=DEV)
+
+
+def _stream():
+    return torch.cuda.current_stream(DEV).cuda_stream
+
+
+def gpu_setup(phase, weight):
+    H, W = phase.shape
+    lib = _lib.load()
+    ph = torch.from_numpy(np.ascontiguousarray(phase, np.float32)).to(DEV)
+    wt = torch.from_numpy(np.ascontiguousarray(weight, np.float32)).to(DEV) if weight is not None else None
+    outs = [torch.empty((H, W), dtype=torch.float32, device=DEV) for _ in range(4)]
+    valid = torch.empty((H, W), dtype=torch.uint8, device=DEV)
+    ws = _ws(H, W)
+    rc = lib.unw_setup_gradients(ph.data_ptr(), wt.data_ptr() if wt is not None else None, H, W,
+                                 *[o.data_ptr() for o in outs], valid.data_ptr(), ws.data_ptr(), ws.numel(),
+                                 _stream())
+    _lib.check(rc)
+    torch.cuda.synchronize()
+    return [o.cpu().numpy() for o in outs] + [valid.cpu().numpy()]
+
+
+def gpu_laplacian(x, wx, wy):
+    H, W = x.shape
+    t = [torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(DEV) for a in (x, wx, wy)]
+    out = torch.empty((H, W), dtype=torch.float32, device=DEV)
+    ws = _ws(H, W)
+    _lib.check(_lib.load().unw_apply_laplacian(t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), H, W,
+                                               out.data_ptr(), ws.data_ptr(), ws.numel(), _stream()))
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def gpu_precond(r):
+    H, W = r.shape
+    t = torch.from_numpy(np.ascontiguousarray(r, np.float32)).to(DEV)
+    out = torch.empty((H, W), dtype=torch.float32, device=DEV)
+    ws = _ws(H, W)
+    _lib.check(_lib.load().unw_apply_preconditioner(t.data_ptr(), H, W, out.data_ptr(), ws.data_ptr(),
+                                                    ws.numel(), _stream()))
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+# ------------------------------------------------------------------ oracle pieces (float64 / float32)
+def ref_precond64(r):
+    H, W = r.shape
+    lam = (2 * np.cos(np.pi * np.arange(H) / H)[:, None] + 2 * np.cos(np.pi * np.arange(W) / W)[None, :] - 4)
+    lam[0, 0] = 1.0
+    t = sfft.dct(sfft.dct(r.astype(np.float64), type=2, axis=1), type=2, axis=0) / lam
+    t = -t
+    t[0, 0] = 0.0
+    return sfft.idct(sfft.idct(t, type=2, axis=0), type=2, axis=1)
+
+
+def ref_laplacian32(x, wx, wy):
+    H, W = x.shape
+    f = np.float32
+    dx = np.zeros((H, W), f)
+    dy = np.zeros((H, W), f)
+    dx[:, :-1] = x[:, 1:] - x[:, :-1]
+    dy[:-1, :] = x[1:, :] - x[:-1, :]
+    dx *= wx
+    dy *= wy
+    res = np.zeros((H, W), f)
+    res[:, 1:] -= dx[:, :-1]
+    res[:, :-1] += dx[:, :-1]
+    res[1:, :] -= dy[:-1, :]
+    res[:-1, :] += dy[:-1, :]
+    return -res
+
+
+def ref_setup(phase, weight):
+    nan = np.isnan(phase)
+    valid = ~nan
+    phi = np.where(nan, 0, phase).astype(np.float32)
+    if weight is None:
+        w = np.subtract(1.0, nan, dtype=np.float32)
+    else:
+        w = weight.astype(np.float32).copy()
+        w[np.isnan(w)] = 0
+        w[nan] = 0
+        w = np.clip(w, 0.01, 1.0)
+    H, W = phase.shape
+    gx = np.zeros((H, W), np.float32)
+    gy = np.zeros((H, W), np.float32)
+    gx[:, :-1] = phi[:, 1:] - phi[:, :-1]
+    gy[:-1, :] = phi[1:, :] - phi[:-1, :]
+    gx = np.arctan2(np.sin(gx), np.cos(gx))
+    gy = np.arctan2(np.sin(gy), np.cos(gy))
+    wx = np.zeros((H, W), np.float32)
+    wy = np.zeros((H, W), np.float32)
+    wx[:, :-1] = (w[:, :-1] + w[:, 1:]) / np.float32(2)
+    wy[:-1, :] = (w[:-1, :] + w[1:, :]) / np.float32(2)
+    wx[:, :-1] *= (valid[:, :-1] & valid[:, 1:])
+    wy[:-1, :] *= (valid[:-1, :] & valid[1:, :])
+    return gx, gy, wx, wy, valid
+
+
+# ------------------------------------------------------------------ operator kernels
+SHAPES = [(64, 64), (37, 50), (128, 96), (17, 257), (1, 7), (5, 1), (3, 5), (1, 1), (200, 131),
+          (1024, 1024), (2600, 4001), (4096, 4096)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_preconditioner_matches_float64_operator(shape):
+    rng = np.random.default_rng(hash(shape) % 2**32)
+    r = rng.standard_normal(shape).astype(np.float32)
+    z = gpu_precond(r)
+    zr = ref_precond64(r)
+    scale = max(np.abs(zr).max(), 1e-30)
+    assert np.abs(z - zr).max() / scale <= 2e-5, np.abs(z - zr).max() / scale
+
+
+@pytest.mark.parametrize("shape", [(64, 64), (37, 50), (1, 9), (9, 1), (513, 1031)])
+def test_laplacian_matches_reference_op_order(shape):
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(shape).astype(np.float32) * 10
+    wx = rng.uniform(1e-6, 2, shape).astype(np.float32)
+    wy = rng.uniform(1e-6, 2, shape).astype(np.float32)
+    a = gpu_laplacian(x, wx, wy)
+    b = ref_laplacian32(x, wx, wy)
+    assert np.abs(a - b).max() <= 1e-6 * max(1.0, np.abs(b).max())
+    assert (a == b).mean() >= 0.999
+
+
+@pytest.mark.parametrize("with_weight", [True, False])
+def test_setup_gradients(with_weight):
+    p, c, _ = gen_g1(96, 120, seed=3)
+    c = c.copy()
+    c[5, 5] = np.nan      # NaN weight on a valid pixel
+    c[6, 6] = 7.0          # clipped to 1
+    c[7, 7] = -1.0         # clipped to 0.01
+    gx, gy, wx, wy, v = gpu_setup(p, c if with_weight else None)
+    rgx, rgy, rwx, rwy, rv = ref_setup(p, c if with_weight else None)
+    assert (v.astype(bool) == rv).all()
+    np.testing.assert_allclose(gx, rgx, atol=2e-6)
+    np.testing.assert_allclose(gy, rgy, atol=2e-6)
+    np.testing.assert_array_equal(wx, rwx)
+    np.testing.assert_array_equal(wy, rwy)
+
+
+# ------------------------------------------------------------------ full solves vs reference outputs
+def _compare(u, cc, ur, ccr, phase, tol_rms=1e-3, min_match=0.9999, exact_cc=True):
+    assert u.dtype == np.float32 and cc.dtype == np.uint16
+    assert (np.isnan(u) == np.isnan(ur)).all()
+    v = np.isfinite(phase)
+    if not v.any():
+        assert (cc == 0).all()
+        return
+    match = (cycle_map(u, phase) == cycle_map(ur, phase))[v].mean()
+    assert match >= min_match, match
+    e = (u.astype(np.float64) - ur)[v]
+    rms = np.sqrt(np.mean((e - e.mean()) ** 2))
+    assert rms <= tol_rms, rms
+    if exact_cc:
+        # identical partition and sizes; labels of equal-size components may differ
+        assert (cc == 0).sum() == (ccr == 0).sum()
+        for lab in np.unique(ccr[ccr > 0]):
+            m = ccr == lab
+            labs = np.unique(cc[m])
+            assert len(labs) == 1 and labs[0] > 0
+            assert (cc == labs[0]).sum() == m.sum()
+
+
+@pytest.mark.parametrize("name", small_golden_names())
+def test_solve_matches_reference_fixture(name):
+    d = load_golden(name)
+    u, cc = core_b200.irls_unwrap_2d(d["phase"], d["w"], **d["kw"])
+    _compare(u, cc, d["u"], d["cc"], d["phase"])
+
+
+@pytest.mark.parametrize("name", ["L_g1_1024_fn_fp32", "L_g1_1024_fn_fp64", "L_g1_1024_api_fp32"])
+def test_solve_1024_matches_reference(name):
+    d = load_golden(name)
+    H, W, seed = [int(x) for x in d["gen_args"]]
+    p, c, _ = gen_g1(H, W, seed=seed)
+    u, cc = core_b200.irls_unwrap_2d(p, c, **d["kw"])
+    v = np.isfinite(p)
+    k = cycle_map(u, p)
+    assert (k == d["cycles"])[v].mean() >= 0.9999
+    s = int(d["step"])
+    us, ps = u[::s, ::s], p[::s, ::s]
+    vs = np.isfinite(ps)
+    e = (us.astype(np.float64) - d["u_sub"])[vs]
+    assert np.sqrt(np.mean((e - e.mean()) ** 2)) <= 1e-3
+    assert np.array_equal(np.bincount(cc.ravel().astype(np.int64), minlength=len(d["cc_hist"]))[:len(d["cc_hist"])],
+                          d["cc_hist"])
+
+
+def test_solve_4096_fault_matches_reference_cycle_map():
+    path = os.path.join(os.path.dirname(__file__), "golden", "L_g2_4096_fn_fp32.npz")
+    if not os.path.exists(path):
+        pytest.skip("4096^2 reference fixture not generated")
+    d = load_golden("L_g2_4096_fn_fp32")
+    p, c, _ = gen_g2(4096, seed=0)
+    u, cc = core_b200.irls_unwrap_2d(p, c, **d["kw"])
+    v = np.isfinite(p)
+    match = (cycle_map(u, p) == d["cycles"])[v].mean()
+    assert match >= 0.9999, match
+
+
+def test_batch_equals_single_solves():
+    grids = [gen_g1(96, 80, seed=11), gen_g1(37, 53, seed=12), gen_g2(128, seed=13), gen_g1(61, 127, seed=14)]
+    ps = [g[0] for g in grids]
+    ws = [g[1] for g in grids]
+    ws[1] = None
+    batch = core_b200.irls_unwrap_2d_batch(ps, ws)
+    for (p, w), (ub, cb) in zip(zip(ps, ws), batch):
+        us, cs = core_b200.irls_unwrap_2d(p, w)
+        _compare(ub, cb, us, cs, p, tol_rms=1e-5)
+
+
+def test_batch_matches_oracle_iteration_counts():
+    p, c, _ = gen_g1(128, 160, seed=21)
+    (u, cc, st), = core_b200.irls_unwrap_2d_batch([p], [c], return_stats=True)
+    from oracle.irls_oracle import OracleStats
+    ost = OracleStats()
+    uo, cco = oracle_unwrap(p, c, stats=ost)
+    assert abs(st["irls_iters"] - ost.irls_iters) <= 1
+    _compare(u, cc, uo, cco, p)
+
+
+# ------------------------------------------------------------------ boundary behaviour
+def test_all_nan_input():
+    p = np.full((9, 7), np.nan, np.float64)
+    u, cc = core_b200.irls_unwrap_2d(p)
+    assert u.dtype == np.float64 and np.isnan(u).all() and (cc == 0).all() and cc.dtype == np.uint16
+
+
+def test_float64_and_noncontiguous_inputs():
+    p, c, _ = gen_g1(80, 70, seed=5)
+    big = np.full((100, 150), np.nan)
+    big[10:90, 20:90] = p
+    view = big[10:90, 20:90]          # non-contiguous float64 view
+    u1, c1 = core_b200.irls_unwrap_2d(view, c.astype(np.float64))
+    u2, c2 = core_b200.irls_unwrap_2d(p, c)
+    _compare(u1, c1, u2, c2, p, tol_rms=1e-5)
+
+
+def test_torch_cuda_input_returns_device_tensors():
+    p, c, _ = gen_g1(64, 64, seed=9)
+    pt = torch.from_numpy(p).to(DEV)
+    ct = torch.from_numpy(c).to(DEV)
+    u, cc = core_b200.irls_unwrap_2d(pt, ct)
+    assert u.is_cuda and cc.is_cuda
+    un, ccn = core_b200.irls_unwrap_2d(p, c)
+    np.testing.assert_array_equal(u.cpu().numpy(), un)
+
+
+def test_congruent_output_rewraps_to_input():
+    p, c, _ = gen_g2(256, seed=3)
+    u, cc = core_b200.irls_unwrap_2d(p, c, congruent=True)
+    v = np.isfinite(p)
+    d = u[v].astype(np.float64) - p[v]
+    assert np.abs(np.arctan2(np.sin(d), np.cos(d))).max() <= 1e-5
+
+
+def test_infinite_weights_are_clipped():
+    p, c, _ = gen_g1(64, 64, seed=2)
+    c = c.copy()
+    c[np.isfinite(c)] = np.inf
+    # infinite weights are clipped to 1 (utils_unwrap2d.py:1238): a normal solve
+    u, cc = core_b200.irls_unwrap_2d(p, c)
+    u1, cc1 = core_b200.irls_unwrap_2d(p, np.where(np.isfinite(c), 1.0, c))
+    assert np.isfinite(u[np.isfinite(p)]).all()
+    np.testing.assert_array_equal(u, u1)
+
+
+def test_zero_iterations_returns_dct_initial_solution():
+    p, c, _ = gen_g1(64, 48, seed=4)
+    u, cc = core_b200.irls_unwrap_2d(p, c, max_iter=0)
+    uo, cco = oracle_unwrap(p, c, max_iter=0)
+    _compare(u, cc, uo, cco, p)
