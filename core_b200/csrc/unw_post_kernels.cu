@@ -165,6 +165,18 @@ __device__ __forceinline__ int uf_find(int* parent, int x) {
     return -1;
 }
 
+// Read-only walk to the root.  The flatten pass must not compress paths: a
+// halving store could overwrite another thread's final parent[x] = root with
+// an intermediate ancestor, leaving a pixel that points at a non-root.
+__device__ __forceinline__ int uf_root(const int* parent, int x) {
+    for (int guard = 0; guard < UNW_UF_LIMIT; guard++) {
+        const int p = __ldcg(&parent[x]);
+        if (p == x) return x;
+        x = p;
+    }
+    return -1;
+}
+
 __device__ __forceinline__ bool uf_union(int* parent, int a, int b) {
     for (int guard = 0; guard < UNW_UF_LIMIT; guard++) {
         a = uf_find(parent, a);
@@ -222,7 +234,8 @@ __global__ void p_union(const GridDev* __restrict__ grids, const int* __restrict
     if (!ok) st->hist_ok = 0;
 }
 
-// One CTA per tile of UNW_TILE_PX pixels: full path compression and root count.
+// One CTA per tile of UNW_TILE_PX pixels: every valid pixel points at its root
+// afterwards (only its own entry is written), and roots are counted per tile.
 __global__ void p_flatten(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
     __shared__ int cnt;
     const int g = find_grid(starts, n, blockIdx.x);
@@ -240,7 +253,7 @@ __global__ void p_flatten(const GridDev* __restrict__ grids, const int* __restri
         const long long q = b0 + t;
         if (q >= npx) break;
         if (G.parent[q] < 0) continue;
-        const int r = uf_find(G.parent, (int)q);
+        const int r = uf_root(G.parent, (int)q);
         if (r < 0) { ok = false; continue; }
         G.parent[q] = r;
         c += (r == (int)q) ? 1 : 0;
@@ -353,6 +366,8 @@ __global__ void p_accum(const GridDev* __restrict__ grids, const int* __restrict
     const long long npx = (long long)G.H * W;
     const float* __restrict__ U = ufinal(G, st);
     const size_t cap = (size_t)G.lab_cap;
+    const int nlab = st->n_labels;
+    bool bad = false;
     for (long long q0 = (long long)local * blockDim.x; q0 < npx; q0 += (long long)nct * blockDim.x) {
         const long long q = q0 + threadIdx.x;
         int L = 0;
@@ -362,6 +377,7 @@ __global__ void p_accum(const GridDev* __restrict__ grids, const int* __restrict
             const size_t o = (size_t)i * P + j;
             if (G.valid[o]) {
                 L = G.lab[G.parent[q]];
+                if (L < 1 || L > nlab) { bad = true; L = 0; }
                 const float ph = G.phase[(long long)i * G.phase_pitch + j];
                 const float u = U[o];
                 si = (double)sinf(ph); ci = (double)cosf(ph);
@@ -400,6 +416,7 @@ __global__ void p_accum(const GridDev* __restrict__ grids, const int* __restrict
             atomicAdd(&G.ccount[L], 1);
         }
     }
+    if (bad) G.st->hist_ok = 0;
 }
 
 // adjust = wrap(circmean(phase) - circmean(u)) per label (utils_unwrap2d.py:1704-1716)
@@ -434,13 +451,15 @@ __global__ void p_write(const GridDev* __restrict__ grids, const int* __restrict
     const int W = G.W, P = G.P;
     const long long npx = (long long)G.H * W;
     const float* __restrict__ U = ufinal(G, st);
+    const int nlab = st->n_labels;
     for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
         const int i = (int)(q / W), j = (int)(q - (long long)i * W);
         const size_t o = (size_t)i * P + j;
         float u = __int_as_float(0x7fc00000);
         uint16_t cc = 0;
         if (G.valid[o]) {
-            const int L = G.parent[q];
+            int L = G.parent[q];
+            L = (L >= 1 && L <= nlab) ? L : 0;
             u = (float)((double)U[o] + G.adj[L]);
             cc = (uint16_t)G.remap[L];
             if (G.congruent) {

@@ -311,3 +311,15 @@ def test_zero_iterations_returns_dct_initial_solution():
     u, cc = core_b200.irls_unwrap_2d(p, c, max_iter=0)
     uo, cco = oracle_unwrap(p, c, max_iter=0)
     _compare(u, cc, uo, cco, p)
+
+
+def test_repeat_calls_on_reused_workspace_are_identical():
+    # the second call reuses the first call's workspace (stale contents must not matter)
+    p, c, _ = gen_g1(1024, seed=0)
+    u1, c1 = core_b200.irls_unwrap_2d(p, c)
+    ws = core_b200.unwrap2d._ws().buf
+    for b in ws.values():
+        b.fill_(0xA5)                       # poison the cached workspace
+    u2, c2 = core_b200.irls_unwrap_2d(p, c)
+    np.testing.assert_array_equal(u1, u2)
+    np.testing.assert_array_equal(c1, c2)
