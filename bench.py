@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark: unwrapped Mpx/s of the B200 DCT+IRLS L1 unwrapper.
+
+Workload (one "step" = one full unwrap, function-default iteration parameters
+max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2):
+  g2_4096   4096 x 4096 float32 grid, G2 generator (Gaussian + ramp truth, 3*pi
+            fault, noise 0.6 rad, Beta(2,2) coherence, 5% NaN ellipses), seed 0.
+            Seeded synthetic input standing in for the reference's benchmark data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    torchrun --nproc-per-node N bench.py --gpus N ...   (one replica per GPU)
+
+Printed JSON (rank 0, one line):
+  value      Mpx/s with inputs resident in HBM (C ABI on device pointers),
+             K solves timed with CUDA events, max over ranks, barrier both sides;
+  e2e        same metric through the public API irls_unwrap_2d with pinned host
+             input and numpy output (H2D + D2H inside the timed region);
+  roofline   dominant kernel's algorithmic bytes / its mean CUDA-event launch
+             time inside the timed region, against MEASURED_PEAKS.json hbm_gbs;
+  cpu_baseline  the numpy oracle on the GPU host's cores, bounded sample;
+  clocks     nvidia-smi samples taken during the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+FN = dict(max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2, conncomp_size=30)
+METRIC = "unwrapped Mpx/s (4096^2 fault grid, function-default iterations)"
+UNIT = "Mpx/s"
+
+# Algorithmic HBM bytes per pixel per launch of each kernel family (float32 words,
+# halo re-reads and reduction partials not counted).
+ALG_BYTES = {
+    "matvec": 24.0,    # read z, p_old, wIx, wIy; write p, Ap
+    "row_upd": 28.0,   # read x, p, r, Ap; write x, r, T
+    "col": 8.0,        # read T; write T
+    "row_inv": 12.0,   # read T, r; write z
+    "head": 40.0,      # read u, gx, gy, wx, wy; write u, wIx, wIy, b (+ halo)
+    "row_r0": 24.0,    # read b, x, wIx, wIy; write r, T
+}
+
+
+def load_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms (background process)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    """torchrun env -> (rank, world, local_rank); initialises NCCL when world > 1."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier_max(x, world, local):
+    """Barrier, then the max of a float over ranks."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=torch.device("cuda", local))
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def make_input(seed=0):
+    from oracle.generators import gen_g2
+    p, c, _ = gen_g2(4096, seed=seed)
+    return p, c
+
+
+# --------------------------------------------------------------------------- CPU baseline
+def cpu_sample(p, c, n_irls, workers):
+    """The oracle on a bounded sample of the workload: the setup + DCT initial
+    solve + post-processing (max_iter=0) and one IRLS iteration of 20 PCG steps;
+    the full-solve time is extrapolated as t0 + n_irls * (t1 - t0), n_irls being
+    the IRLS count of the same solve (identical algorithm)."""
+    from oracle.irls_oracle import irls_unwrap_2d as oracle
+    kw = dict(FN)
+    t = time.perf_counter()
+    oracle(p, c, workers=workers, **dict(kw, max_iter=0))
+    t0 = time.perf_counter() - t
+    t = time.perf_counter()
+    oracle(p, c, workers=workers, **dict(kw, max_iter=1, tol=0.0))
+    t1 = time.perf_counter() - t
+    full = t0 + n_irls * max(t1 - t0, 0.0)
+    return t0, t1, full
+
+
+def run_reference(args):
+    """--impl reference: the oracle restatement of the reference's CPU path."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    workers = os.cpu_count()
+    p, c = make_input()
+    npx = p.size
+    n_irls = 30  # IRLS iterations of this solve under function defaults (reference CPU run)
+    from oracle.irls_oracle import irls_unwrap_2d as oracle
+    t = time.perf_counter()
+    oracle(p, c, workers=workers, **dict(FN, max_iter=0))
+    t0 = time.perf_counter() - t
+    samples = []
+    for i in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        oracle(p, c, workers=workers, **dict(FN, max_iter=1, tol=0.0))
+        dt = time.perf_counter() - t
+        if i >= args.warmup:
+            samples.append(max(dt - t0, 1e-9))
+    t_irls = float(np.median(samples))
+    full = t0 + n_irls * t_irls
+    value = npx / 1e6 / full
+    sample = (f"per step: 1 IRLS iteration (20 PCG) of the 4096^2 solve; full solve = "
+              f"init+post {t0:.1f}s + {n_irls} x {t_irls:.1f}s")
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": full * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+           "config": {"workload": "g2_4096 fn-defaults", "grid": [4096, 4096], "params": FN},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- GPU arm
+def run_b200(args):
+    import torch
+
+    import core_b200
+    from core_b200 import _lib
+    from core_b200.unwrap2d import make_params
+
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    p, c = make_input(seed=rank)
+    H, W = p.shape
+    npx = H * W
+
+    ph = torch.from_numpy(p).to(dev)
+    wt = torch.from_numpy(c).to(dev)
+    out_u = torch.empty((H, W), dtype=torch.float32, device=dev)
+    out_cc = torch.empty((H, W), dtype=torch.int16, device=dev)
+    ws = torch.empty(lib.unw_workspace_bytes(H, W), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def solve(flags=0):
+        prm = make_params(**FN)
+        prm.flags |= flags
+        st = _lib.UnwStats()
+        rc = lib.unw_solve_f32(ph.data_ptr(), W, wt.data_ptr(), W, H, W, C.byref(prm), out_u.data_ptr(), W,
+                               out_cc.data_ptr(), W, ws.data_ptr(), ws.numel(), C.byref(st), stream.cuda_stream)
+        _lib.check(rc, "unw_solve_f32")
+        return st
+
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+
+    # ---- device-resident timed region (per-kernel CUDA events on the solve stream)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    prof_ms = np.zeros(_lib.PROF_N)
+    prof_n = np.zeros(_lib.PROF_N, dtype=np.int64)
+    stats = None
+    for _ in range(args.steps):
+        st = solve(_lib.UNW_F_PROFILE)
+        prof_ms += np.array(st.prof_ms[:_lib.PROF_N])
+        prof_n += np.array(st.prof_launches[:_lib.PROF_N])
+        stats = st.as_dict()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    t_dev = ev0.elapsed_time(ev1) / 1e3
+    t_dev = barrier_max(t_dev, world, local)
+    value = world * npx * args.steps / 1e6 / t_dev
+
+    # ---- end to end through the public API: pinned host input, numpy output
+    pin_p = torch.from_numpy(p).pin_memory()
+    pin_c = torch.from_numpy(c).pin_memory()
+    for _ in range(1):
+        core_b200.irls_unwrap_2d(pin_p, pin_c, device=dev, **FN)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_steps = max(1, min(args.steps, 3))
+    t = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(e2e_steps):
+        u_np, cc_np = core_b200.irls_unwrap_2d(pin_p, pin_c, device=dev, **FN)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = max(ev0.elapsed_time(ev1) / 1e3, time.perf_counter() - t)
+    barrier(world)
+    t_e2e = barrier_max(t_e2e, world, local)
+    e2e = world * npx * e2e_steps / 1e6 / t_e2e
+
+    # ---- roofline of the dominant kernel (live event times from the timed region)
+    names = _lib.PROF_NAMES
+    peak, peak_kind = load_peaks()
+    fam = {names[i]: (prof_ms[i], prof_n[i]) for i in range(len(names))}
+    dom = max(ALG_BYTES, key=lambda k: fam[k][0])
+    ms, n = fam[dom]
+    per_launch_s = ms / 1e3 / max(n, 1)
+    achieved = ALG_BYTES[dom] * npx / per_launch_s / 1e9
+    kernels = {}
+    for k in ALG_BYTES:
+        kms, kn = fam[k]
+        if kn:
+            kernels[k] = {"launches": int(kn), "ms_total": round(float(kms), 3),
+                          "us_per_launch": round(float(kms) / kn * 1e3, 2),
+                          "gbs": round(ALG_BYTES[k] * npx / (kms / 1e3 / kn) / 1e9, 1)}
+    pcg_ms = sum(fam[k][0] for k in ("matvec", "row_upd", "col", "row_inv"))
+    n_pcg = max(int(fam["matvec"][1]), 1)
+    traffic = None
+    tf = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(dom)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": dom,
+                "peak_source": peak_kind,
+                "alg_bytes_per_launch": ALG_BYTES[dom] * npx,
+                "pcg_iteration": {"us": round(pcg_ms / n_pcg * 1e3, 1), "alg_bytes_per_px": 72.0,
+                                  "gbs": round(72.0 * npx / (pcg_ms / 1e3 / n_pcg) / 1e9, 1)},
+                "kernels": kernels}
+
+    # ---- CPU baseline (rank 0, N=1 only): the oracle on a bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        workers = os.cpu_count()
+        t0, t1, full = cpu_sample(p, c, stats["irls_iters"], workers)
+        cpu = {"value": round(npx / 1e6 / full, 5), "unit": UNIT, "cores": workers, "kind": "port",
+               "sample": (f"oracle (numpy/scipy.fft, {workers} threads) on the same 4096^2 input: "
+                          f"max_iter=0 run {t0:.1f}s + one IRLS iteration (20 PCG) {t1 - t0:.1f}s, "
+                          f"extrapolated to {stats['irls_iters']} IRLS iterations = {full:.0f}s")}
+
+    launches = int(prof_n.sum())
+    out = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(t_dev / args.steps * 1e3, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "g2_4096 fn-defaults (one full unwrap per step, replica per GPU)",
+                      "grid": [H, W], "params": FN, "irls_iters": stats["irls_iters"],
+                      "pcg_iters": stats["cg_iters_total"],
+                      "l2": "inputs 134 MB and solver working set ~1.1 GB exceed the 126 MB L2",
+                      "parallelism": f"replicas x{world}"},
+           "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(npx * 8),
+                   "d2h_bytes_per_step": int(npx * 6)},
+           "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches // 1}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -22,6 +22,10 @@ UNW_E_OVERFLOW = -5
 
 UNW_F_CONGRUENT = 1
 UNW_F_NO_GRAPH = 2
+UNW_F_PROFILE = 4
+
+PROF_NAMES = ["bbox", "setup", "row_rho", "col", "row_inv", "matvec", "row_upd", "row_r0", "head", "elem", "post"]
+PROF_N = len(PROF_NAMES)
 
 UNW_S_DCT_INIT_NONFINITE = 1
 UNW_S_REVERTED = 2
@@ -39,7 +43,8 @@ class UnwStats(C.Structure):
     _fields_ = [("irls_iters", C.c_int32), ("cg_iters_total", C.c_int32), ("cg_iters_last", C.c_int32),
                 ("n_components", C.c_int32), ("n_labels", C.c_int32), ("status", C.c_int32),
                 ("bbox", C.c_int32 * 4), ("rel_change", C.c_double), ("best_residual", C.c_double),
-                ("k_median", C.c_double), ("cg_iters", C.c_int32 * 64)]
+                ("k_median", C.c_double), ("cg_iters", C.c_int32 * 64),
+                ("prof_ms", C.c_float * 16), ("prof_launches", C.c_int32 * 16)]
 
     def as_dict(self):
         n = min(self.irls_iters, 64)
@@ -47,7 +52,8 @@ class UnwStats(C.Structure):
                     cg_iters_last=self.cg_iters_last, n_components=self.n_components,
                     n_labels=self.n_labels, status=self.status, bbox=tuple(self.bbox),
                     rel_change=self.rel_change, best_residual=self.best_residual,
-                    k_median=self.k_median, cg_iters=list(self.cg_iters[:n]))
+                    k_median=self.k_median, cg_iters=list(self.cg_iters[:n]),
+                    prof_ms=list(self.prof_ms[:PROF_N]), prof_launches=list(self.prof_launches[:PROF_N]))
 
 
 class UnwGrid(C.Structure):

@@ -40,6 +40,14 @@ int set_err(int code, const char* fmt, ...) {
             return set_err(UNW_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));  \
     } while (0)
 
+// a kernel launch of family `fam`, timed when profiling is on
+#define PL(fam, call)              \
+    do {                           \
+        S.prof.begin((fam), S.s);  \
+        CK(call);                  \
+        S.prof.end(S.s);           \
+    } while (0)
+
 constexpr int EMAX = 16;
 constexpr size_t ALIGN = 256;
 constexpr int HIST_CAP = 65536;
@@ -193,8 +201,53 @@ int elem_ctas(long long npx) {
     return (int)std::max<long long>(1, std::min<long long>(c, ELEM_MAX_CTAS));
 }
 
+// Optional per-launch CUDA-event timing (UNW_F_PROFILE): an event pair brackets
+// each kernel launch on the solve stream; times are summed per kernel family.
+struct Prof {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    std::vector<std::pair<int, size_t>> marks;  // (family, index of the start event)
+    size_t next = 0;
+    int fam = 0;
+    size_t cur = 0;
+    cudaEvent_t get() {
+        if (next == pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            pool.push_back(e);
+        }
+        return pool[next++];
+    }
+    void begin(int f, cudaStream_t s) {
+        if (!on) return;
+        fam = f;
+        cur = next;
+        cudaEventRecord(get(), s);
+    }
+    void end(cudaStream_t s) {
+        if (!on) return;
+        cudaEventRecord(get(), s);
+        marks.push_back({fam, cur});
+    }
+    void collect(float* ms, int* cnt) {
+        if (!on) return;
+        for (auto& m : marks) {
+            float t = 0.f;
+            if (cudaEventSynchronize(pool[m.second + 1]) == cudaSuccess &&
+                cudaEventElapsedTime(&t, pool[m.second], pool[m.second + 1]) == cudaSuccess) {
+                ms[m.first] += t;
+                cnt[m.first] += 1;
+            }
+        }
+    }
+    ~Prof() {
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
 struct Solver {
     int n = 0;
+    Prof prof;
     cudaStream_t s = nullptr;
     std::vector<GridDev> hg;     // host copies
     std::vector<int> starts;     // [KS_NKIND + 1][n + 1]  (last row: post tiles)
@@ -223,19 +276,19 @@ int kind_ctas(const GridDev& G, int kind) {
 int enqueue_iteration(Solver& S, int t) {
     const int n = S.n;
     cudaStream_t s = S.s;
-    CK(unw_launch_simple(UNW_K_MEAN, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
-    CK(unw_launch_simple(UNW_K_HEAD, S.total[KS_STEN], s, S.dg, S.ds(KS_STEN), n, t, S.sc));
-    CK(unw_launch_simple(UNW_K_COPY_BEST, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
-    CK(unw_launch_row_fwd(1, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, t, 0));
-    CK(unw_launch_col(1, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
-    CK(unw_launch_row_inv(1, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
+    PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_MEAN, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
+    PL(UNW_PROF_HEAD, unw_launch_simple(UNW_K_HEAD, S.total[KS_STEN], s, S.dg, S.ds(KS_STEN), n, t, S.sc));
+    PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_COPY_BEST, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
+    PL(UNW_PROF_ROW_R0, unw_launch_row_fwd(1, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, t, 0));
+    PL(UNW_PROF_COL, unw_launch_col(1, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
+    PL(UNW_PROF_ROW_INV, unw_launch_row_inv(1, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
     for (int k = 0; k < S.sc.cg_max_iter; k++) {
-        CK(unw_launch_simple(UNW_K_MATVEC, S.total[KS_STEN], s, S.dg, S.ds(KS_STEN), n, k, S.sc));
-        CK(unw_launch_row_fwd(2, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, t, k));
-        CK(unw_launch_col(1, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
-        CK(unw_launch_row_inv(2, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
+        PL(UNW_PROF_MATVEC, unw_launch_simple(UNW_K_MATVEC, S.total[KS_STEN], s, S.dg, S.ds(KS_STEN), n, k, S.sc));
+        PL(UNW_PROF_ROW_UPD, unw_launch_row_fwd(2, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, t, k));
+        PL(UNW_PROF_COL, unw_launch_col(1, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
+        PL(UNW_PROF_ROW_INV, unw_launch_row_inv(2, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
     }
-    CK(unw_launch_simple(UNW_K_REL, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
+    PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_REL, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
     return UNW_OK;
 }
 
@@ -426,18 +479,19 @@ int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, s
     CK(cudaStreamSynchronize(s));
 
     Solver S;
+    S.prof.on = (prm->flags & UNW_F_PROFILE) != 0;
     rc = prepare(S, n, grids, bbox, prm, base, B, s, false);
     if (rc) return rc;
 
     // 4. setup and DCT initial solve (utils_unwrap2d.py:1228-1513)
     const int tot_active = S.total[KS_ROWPAIR];
-    CK(unw_launch_simple(UNW_K_STATE_INIT, 1, s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
+    PL(UNW_PROF_SETUP, unw_launch_simple(UNW_K_STATE_INIT, 1, s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
     if (tot_active > 0) {
-        CK(unw_launch_simple(UNW_K_SETUP, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
-        CK(unw_launch_row_fwd(0, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, 0, 0));
-        CK(unw_launch_col(0, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
-        CK(unw_launch_row_inv(0, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
-        CK(unw_launch_simple(UNW_K_INIT_RECENTRE, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
+        PL(UNW_PROF_SETUP, unw_launch_simple(UNW_K_SETUP, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
+        PL(UNW_PROF_ROW_RHO, unw_launch_row_fwd(0, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, 0, 0));
+        PL(UNW_PROF_COL, unw_launch_col(0, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
+        PL(UNW_PROF_ROW_INV, unw_launch_row_inv(0, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
+        PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_INIT_RECENTRE, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
 
         // 5. IRLS loop (utils_unwrap2d.py:1533-1626)
         const int every = std::max(1, prm->check_every);
@@ -455,16 +509,16 @@ int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, s
         }
 
         // 6. post-processing (utils_unwrap2d.py:1659-1757)
-        CK(unw_launch_post(UNW_P_KSTATS, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
-        CK(unw_launch_post(UNW_P_HIST, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
-        CK(unw_launch_post(UNW_P_MEDIAN, n, s, S.dg, nullptr, n, S.sc, S.hg.data()));
-        CK(unw_launch_post(UNW_P_SHIFT_CCINIT, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
-        CK(unw_launch_post(UNW_P_UNION, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
-        CK(unw_launch_post(UNW_P_FLATTEN, S.total[KS_NKIND], s, S.dg, S.ds(KS_NKIND), n, S.sc, S.hg.data()));
-        CK(unw_launch_post(UNW_P_TILESCAN, n, s, S.dg, nullptr, n, S.sc, S.hg.data()));
-        CK(unw_launch_post(UNW_P_LABEL, S.total[KS_NKIND], s, S.dg, S.ds(KS_NKIND), n, S.sc, S.hg.data()));
-        CK(unw_launch_post(UNW_P_ACCUM, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
-        CK(unw_launch_post(UNW_P_ADJUST, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        PL(UNW_PROF_POST, unw_launch_post(UNW_P_KSTATS, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        PL(UNW_PROF_POST, unw_launch_post(UNW_P_HIST, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        PL(UNW_PROF_POST, unw_launch_post(UNW_P_MEDIAN, n, s, S.dg, nullptr, n, S.sc, S.hg.data()));
+        PL(UNW_PROF_POST, unw_launch_post(UNW_P_SHIFT_CCINIT, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        PL(UNW_PROF_POST, unw_launch_post(UNW_P_UNION, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        PL(UNW_PROF_POST, unw_launch_post(UNW_P_FLATTEN, S.total[KS_NKIND], s, S.dg, S.ds(KS_NKIND), n, S.sc, S.hg.data()));
+        PL(UNW_PROF_POST, unw_launch_post(UNW_P_TILESCAN, n, s, S.dg, nullptr, n, S.sc, S.hg.data()));
+        PL(UNW_PROF_POST, unw_launch_post(UNW_P_LABEL, S.total[KS_NKIND], s, S.dg, S.ds(KS_NKIND), n, S.sc, S.hg.data()));
+        PL(UNW_PROF_POST, unw_launch_post(UNW_P_ACCUM, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        PL(UNW_PROF_POST, unw_launch_post(UNW_P_ADJUST, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
         // size-ranked relabel (utils_unwrap2d.py:1722-1746): sizes to the host, sorted there
         rc = read_states(S, hs);
         if (rc) return rc;
@@ -489,9 +543,9 @@ int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, s
             CK(cudaMemcpyAsync(G.remap, remap.data(), sizeof(int) * (nl + 1), cudaMemcpyHostToDevice, s));
             if (stats) stats[g].n_components = nw - 1;
         }
-        CK(unw_launch_post(UNW_P_WRITE, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+        PL(UNW_PROF_POST, unw_launch_post(UNW_P_WRITE, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
     }
-    CK(unw_launch_post(UNW_P_FILL, 0, s, S.dg, nullptr, n, S.sc, S.hg.data()));
+    PL(UNW_PROF_POST, unw_launch_post(UNW_P_FILL, 0, s, S.dg, nullptr, n, S.sc, S.hg.data()));
     std::vector<InstState> fin;
     rc = read_states(S, fin);
     if (rc) return rc;
@@ -523,6 +577,7 @@ int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, s
             for (int i = 0; i < 64 && i < UNW_MAX_LOG; i++) o.cg_iters[i] = G.H ? st.cg_log[i] : 0;
         }
     }
+    if (stats && S.prof.on) S.prof.collect(stats[0].prof_ms, stats[0].prof_launches);
     return ret;
 }
 

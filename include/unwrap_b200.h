@@ -56,6 +56,14 @@ typedef struct unw_params {
 
 #define UNW_F_CONGRUENT 1   /* output phase + 2*pi*k instead of the smooth solution */
 #define UNW_F_NO_GRAPH  2   /* launch kernels one by one instead of a CUDA graph    */
+#define UNW_F_PROFILE   4   /* time every kernel launch with CUDA events (unw_stats.prof_*) */
+
+/* Kernel families timed under UNW_F_PROFILE (index into unw_stats.prof_*). */
+enum {
+    UNW_PROF_BBOX = 0, UNW_PROF_SETUP, UNW_PROF_ROW_RHO, UNW_PROF_COL, UNW_PROF_ROW_INV,
+    UNW_PROF_MATVEC, UNW_PROF_ROW_UPD, UNW_PROF_ROW_R0, UNW_PROF_HEAD, UNW_PROF_ELEM,
+    UNW_PROF_POST, UNW_PROF_N
+};
 
 /* Per-solve statistics (the reference prints these under debug=True). */
 typedef struct unw_stats {
@@ -70,6 +78,8 @@ typedef struct unw_stats {
     double best_residual;   /* best sum of squared gradient residuals            */
     double k_median;        /* median 2-pi cycle shift applied                   */
     int32_t cg_iters[64];   /* PCG iterations of the first 64 IRLS iterations    */
+    float prof_ms[16];      /* summed kernel time per family (UNW_F_PROFILE)     */
+    int32_t prof_launches[16]; /* launches per family (UNW_F_PROFILE)            */
 } unw_stats;
 
 #define UNW_S_DCT_INIT_NONFINITE 1   /* DCT init produced NaN/inf (zero-filled)  */
