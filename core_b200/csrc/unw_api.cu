@@ -133,7 +133,8 @@ GridLayout grid_layout(long long H0, long long W0) {
     auto take = [&](size_t bytes) { size_t r = o; o = up(o + bytes, ALIGN); return r; };
     L.P0 = (long long)up((size_t)W0, 32);
     const size_t A = (size_t)H0 * (size_t)L.P0 * sizeof(float);
-    L.max_ctas = std::max<long long>({(H0 + 1) / 2, (W0 + 1) / 2, ((W0 + 255) / 256) * H0, ELEM_MAX_CTAS});
+    L.max_ctas = std::max<long long>({(H0 + 1) / 2, (W0 + 1) / 2, ((W0 + 127) / 128) * ((H0 + 15) / 16),
+                                      ELEM_MAX_CTAS});
     L.fr_cap = (int)std::max<long long>(next_smooth(2 * W0 - 1), W0);
     L.fc_cap = (int)std::max<long long>(next_smooth(2 * H0 - 1), H0);
     L.st = take(sizeof(InstState));
@@ -194,6 +195,7 @@ BatchLayout batch_layout(int n, const long long* H, const long long* W) {
 struct Shape {
     int row_T = 0, col_T = 0;
     size_t row_smem = 0, col_smem = 0;
+    int row_p2 = 0, col_p2 = 0;   // power-of-two register-FFT paths (length), 0 = generic
 };
 
 int elem_ctas(long long npx) {
@@ -265,11 +267,28 @@ int kind_ctas(const GridDev& G, int kind) {
     switch (kind) {
         case KS_ROWPAIR: return (G.H + 1) / 2;
         case KS_COL: return (G.W + 2 * G.col_nseq - 1) / (2 * G.col_nseq);
-        case KS_STEN: return G.sten_tiles_x * ((G.H + G.sten_rows - 1) / G.sten_rows);
+        case KS_STEN: return G.sten_tiles_x * ((G.H + 8 * G.sten_rows - 1) / (8 * G.sten_rows));
         case KS_ELEM: return elem_ctas(npx);
         case KS_ONE: return 1;
         default: return (int)((npx + 4095) / 4096);  // post tiles
     }
+}
+
+// DCT pass launchers: power-of-two register-FFT kernels or the generic ones
+cudaError_t L_rowf(Solver& S, int mode, int it, int cgk) {
+    if (S.sh.row_p2)
+        return unw_launch_rowf_p2(S.sh.row_p2, mode, S.total[KS_ROWPAIR], S.s, S.dg, S.ds(KS_ROWPAIR), S.n, it, cgk);
+    return unw_launch_row_fwd(mode, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg,
+                              S.ds(KS_ROWPAIR), S.n, it, cgk);
+}
+cudaError_t L_rowi(Solver& S, int mode) {
+    if (S.sh.row_p2) return unw_launch_rowi_p2(S.sh.row_p2, mode, S.total[KS_ROWPAIR], S.s, S.dg, S.ds(KS_ROWPAIR), S.n);
+    return unw_launch_row_inv(mode, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg,
+                              S.ds(KS_ROWPAIR), S.n);
+}
+cudaError_t L_col(Solver& S, int mode) {
+    if (S.sh.col_p2) return unw_launch_col_p2(S.sh.col_p2, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n);
+    return unw_launch_col(mode, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, S.s, S.dg, S.ds(KS_COL), S.n);
 }
 
 // ------------------------------------------------------------ IRLS enqueue
@@ -279,14 +298,14 @@ int enqueue_iteration(Solver& S, int t) {
     PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_MEAN, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
     PL(UNW_PROF_HEAD, unw_launch_simple(UNW_K_HEAD, S.total[KS_STEN], s, S.dg, S.ds(KS_STEN), n, t, S.sc));
     PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_COPY_BEST, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
-    PL(UNW_PROF_ROW_R0, unw_launch_row_fwd(1, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, t, 0));
-    PL(UNW_PROF_COL, unw_launch_col(1, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
-    PL(UNW_PROF_ROW_INV, unw_launch_row_inv(1, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
+    PL(UNW_PROF_ROW_R0, L_rowf(S, 1, t, 0));
+    PL(UNW_PROF_COL, L_col(S, 1));
+    PL(UNW_PROF_ROW_INV, L_rowi(S, 1));
     for (int k = 0; k < S.sc.cg_max_iter; k++) {
         PL(UNW_PROF_MATVEC, unw_launch_simple(UNW_K_MATVEC, S.total[KS_STEN], s, S.dg, S.ds(KS_STEN), n, k, S.sc));
-        PL(UNW_PROF_ROW_UPD, unw_launch_row_fwd(2, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, t, k));
-        PL(UNW_PROF_COL, unw_launch_col(1, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
-        PL(UNW_PROF_ROW_INV, unw_launch_row_inv(2, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
+        PL(UNW_PROF_ROW_UPD, L_rowf(S, 2, t, k));
+        PL(UNW_PROF_COL, L_col(S, 1));
+        PL(UNW_PROF_ROW_INV, L_rowi(S, 2));
     }
     PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_REL, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
     return UNW_OK;
@@ -403,8 +422,24 @@ int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbo
         S.sh.col_T = std::max(S.sh.col_T, cT);
         S.sh.row_smem = std::max(S.sh.row_smem, (size_t)prow[g].n * sizeof(float2));
         S.sh.col_smem = std::max(S.sh.col_smem, (size_t)nseq * pcol[g].n * sizeof(float2));
-        G.sten_tiles_x = (G.W + 255) / 256;
-        G.sten_rows = (int)std::max<long long>(1, std::min<long long>(32, (long long)G.sten_tiles_x * G.H / 592));
+        G.sten_tiles_x = (G.W + 127) / 128;
+        G.sten_rows = (int)std::max<long long>(2, std::min<long long>(16, (long long)G.sten_tiles_x * G.H / 4800));
+    }
+    // power-of-two register-FFT paths when every grid shares the dimension
+    {
+        int w = -1, h = -1;
+        bool wsame = true, hsame = true;
+        for (int g = 0; g < n; g++) {
+            const GridDev& G = S.hg[g];
+            if (G.H == 0) continue;
+            if (w < 0) w = G.W; else wsame &= (w == G.W);
+            if (h < 0) h = G.H; else hsame &= (h == G.H);
+        }
+        if (w > 0 && wsame && unw_p2_col_nseq(w) > 0 && (w & (w - 1)) == 0) S.sh.row_p2 = w;
+        if (h > 0 && hsame && unw_p2_col_nseq(h) > 0 && (h & (h - 1)) == 0) {
+            S.sh.col_p2 = h;
+            for (int g = 0; g < n; g++) S.hg[g].col_nseq = unw_p2_col_nseq(h);
+        }
     }
     // CTA prefix arrays
     S.starts.assign((size_t)(KS_NKIND + 1) * (n + 1), 0);
@@ -488,9 +523,9 @@ int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, s
     PL(UNW_PROF_SETUP, unw_launch_simple(UNW_K_STATE_INIT, 1, s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
     if (tot_active > 0) {
         PL(UNW_PROF_SETUP, unw_launch_simple(UNW_K_SETUP, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
-        PL(UNW_PROF_ROW_RHO, unw_launch_row_fwd(0, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n, 0, 0));
-        PL(UNW_PROF_COL, unw_launch_col(0, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, s, S.dg, S.ds(KS_COL), n));
-        PL(UNW_PROF_ROW_INV, unw_launch_row_inv(0, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, s, S.dg, S.ds(KS_ROWPAIR), n));
+        PL(UNW_PROF_ROW_RHO, L_rowf(S, 0, 0, 0));
+        PL(UNW_PROF_COL, L_col(S, 0));
+        PL(UNW_PROF_ROW_INV, L_rowi(S, 0));
         PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_INIT_RECENTRE, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
 
         // 5. IRLS loop (utils_unwrap2d.py:1533-1626)
@@ -694,9 +729,9 @@ int unw_apply_preconditioner(const float* r, int64_t H, int64_t W, float* z, voi
     G.r = const_cast<float*>(r); G.z = z;
     rc = op_upload(S);
     if (rc) return rc;
-    CK(unw_launch_row_fwd(3, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg, S.ds(KS_ROWPAIR), 1, 0, 0));
-    CK(unw_launch_col(0, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, S.s, S.dg, S.ds(KS_COL), 1));
-    CK(unw_launch_row_inv(3, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg, S.ds(KS_ROWPAIR), 1));
+    CK(L_rowf(S, 3, 0, 0));
+    CK(L_col(S, 0));
+    CK(L_rowi(S, 3));
     return UNW_OK;
 }
 

@@ -37,6 +37,15 @@ cudaError_t unw_launch_col(int mode, int T, int emax, int nblk, size_t smem, cud
 cudaError_t unw_launch_simple(int which, int nblk, cudaStream_t s, const GridDev* gd,
                               const int* starts, int n, int it, UnwScalars sc);
 
+// power-of-two register-FFT DCT passes (N = 256 .. 16384)
+int unw_p2_col_nseq(int N);
+cudaError_t unw_launch_rowf_p2(int N, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
+                               int n, int it, int cgk);
+cudaError_t unw_launch_rowi_p2(int N, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
+                               int n);
+cudaError_t unw_launch_col_p2(int N, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
+                              int n);
+
 // bounding box of valid pixels on the caller's full grid
 cudaError_t unw_launch_bbox(const float* phase, long long pitch, int H0, int W0, int* rowany,
                             int* colany, int* bbox, cudaStream_t s);

@@ -1,0 +1,92 @@
+// Register-resident Stockham FFT for power-of-two lengths N (256..16384).
+//
+// N/16 threads cooperate on one sequence; thread t holds the 16 elements
+// x[t + (N/16) q], q = 0..15, on entry, and X[t + (N/16) q] on exit (the same
+// "stride-T" layout, so the first pass reads registers and the last pass
+// leaves the spectrum in registers).  Passes are radix 16 except a final
+// radix 2/4/8 pass when log2(N) is not a multiple of 4.  Between passes the
+// data goes through shared memory with one padding slot per 16 entries, which
+// makes every exchange pattern free of bank conflicts for 8-byte accesses.
+// Everything is resolved at compile time: no integer division, no dynamic
+// register indexing.
+#pragma once
+#include "unw_fft.cuh"
+
+__device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
+
+constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
+
+template <int N>
+struct RegFft {
+    static_assert((N & (N - 1)) == 0 && N >= 256 && N <= 16384, "power of two in [256, 16384]");
+    static constexpr int LOG = ilog2c(N);
+    static constexpr int T = N / 16;              // threads per sequence
+    static constexpr int NP16 = LOG / 4;          // radix-16 passes
+    static constexpr int REM = LOG % 4;           // log2 of the final small radix (0 = none)
+    static constexpr int NPASS = NP16 + (REM ? 1 : 0);
+    static constexpr int SMEM = N + N / 16;       // float2 slots per sequence
+};
+
+// One Stockham pass of radix R with NS = product of earlier radices.
+// Butterfly j = t + b*T (b < 16/R) reads elements j + r*(N/R) and writes
+// (j - k)*R + k + r*NS, k = j mod NS.
+template <int N, int R, int NS, bool FIRST, bool LAST>
+__device__ __forceinline__ void reg_pass(float2 (&v)[16], float2* __restrict__ sm, int t,
+                                         const float2* __restrict__ tw) {
+    constexpr int T = N / 16;
+    constexpr int NB = 16 / R;
+    constexpr int NR = N / R;
+    constexpr int S = N / (NS * R);
+    float2 w[NB][R];
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            if (FIRST) w[b][r] = v[b + r * NB];
+            else w[b][r] = sm[pad16(t + b * T + r * NR)];
+        }
+    }
+    if (!FIRST) __syncthreads();  // every read of this exchange done before it is overwritten
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        const int j = t + b * T;
+        const int k = j & (NS - 1);
+        if (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; r++) w[b][r] = cmul(w[b][r], __ldg(&tw[r * k * S]));
+        }
+        Dft<R>::run(w[b]);
+        if (LAST) {
+#pragma unroll
+            for (int r = 0; r < R; r++) v[b + r * NB] = w[b][r];
+        } else {
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; r++) sm[pad16(base + r * NS)] = w[b][r];
+        }
+    }
+    if (!LAST) __syncthreads();
+}
+
+template <int N, int P, int NS>
+__device__ __forceinline__ void reg_fft_rec(float2 (&v)[16], float2* sm, int t, const float2* tw) {
+    if constexpr (P < RegFft<N>::NPASS) {
+        constexpr int R = (P < RegFft<N>::NP16) ? 16 : (1 << RegFft<N>::REM);
+        reg_pass<N, R, NS, P == 0, P == RegFft<N>::NPASS - 1>(v, sm, t, tw);
+        reg_fft_rec<N, P + 1, NS * R>(v, sm, t, tw);
+    }
+}
+
+// Forward FFT (exp(-2 pi i nk/N)) in place in the stride-T register layout.
+// `sm` (RegFft<N>::SMEM float2) must not be read by other threads of this
+// sequence while the call runs; the caller synchronises before reusing it.
+template <int N>
+__device__ __forceinline__ void reg_fft(float2 (&v)[16], float2* sm, int t, const float2* tw) {
+    reg_fft_rec<N, 0, 1>(v, sm, t, tw);
+}
+
+// FFT position m of the Makhoul reordering holds source sample n(m).
+template <int N>
+__device__ __forceinline__ int mk_src(int m) {
+    return m < N / 2 ? 2 * m : 2 * N - 1 - 2 * m;
+}

@@ -1,0 +1,149 @@
+// Elementwise work fused into the DCT row passes, shared by the generic and
+// the power-of-two kernels: the value a row-forward pass transforms, what a
+// row-inverse pass does with the transformed value, and the scalar decisions
+// the last CTA of each pass takes (the reference's PCG `break` tests).
+#pragma once
+#include "unw_internal.cuh"
+
+// A x at (i, j): -div(w grad x) in the reference's op order (utils_unwrap2d.py:1367-1388):
+// res = 0; res -= dx[j-1]; res += dx[j]; res -= dy[i-1]; res += dy[i]; Ax = -res.
+__device__ __forceinline__ float lap_at(const float* __restrict__ x, const float* __restrict__ wx,
+                                        const float* __restrict__ wy, int i, int j, int H, int W, int P) {
+    const size_t o = (size_t)i * P + j;
+    const float xc = x[o];
+    float res = 0.f;
+    if (j > 0) res = fsub(res, fmul(fsub(xc, x[o - 1]), wx[o - 1]));
+    if (j < W - 1) res = fadd(res, fmul(fsub(x[o + 1], xc), wx[o]));
+    if (i > 0) res = fsub(res, fmul(fsub(xc, x[o - P]), wy[o - P]));
+    if (i < H - 1) res = fadd(res, fmul(fsub(x[o + P], xc), wy[o]));
+    return -res;
+}
+
+// Row-forward modes:
+//  0 RHO  rho = -div(w g), the DCT initial solve (utils_unwrap2d.py:1478-1483)
+//  1 R0   r = b - A x0, PCG start (utils_unwrap2d.py:1413-1419)
+//  2 UPD  x += alpha p; r -= alpha Ap (utils_unwrap2d.py:1445-1459)
+//  3 COPY r as given (operator entry point)
+template <int MODE>
+__device__ __forceinline__ bool rowfwd_gate(const InstState* s) {
+    if (MODE == 0 || MODE == 3) return true;
+    if (MODE == 1) return s->irls_active != 0;
+    return s->irls_active != 0 && s->cg_active != 0;
+}
+
+template <int MODE>
+__device__ __forceinline__ float rowfwd_value(const GridDev& G, float* __restrict__ U, const float* __restrict__ pk,
+                                              float alpha, int i, int j, double (&acc)[2]) {
+    const int H = G.H, W = G.W, P = G.P;
+    const size_t o = (size_t)i * P + j;
+    if (MODE == 0) {
+        float rr = 0.f;
+        if (j > 0) rr = fadd(rr, fmul(G.wx[o - 1], G.gx[o - 1]));
+        if (j < W - 1) rr = fsub(rr, fmul(G.wx[o], G.gx[o]));
+        if (i > 0) rr = fadd(rr, fmul(G.wy[o - P], G.gy[o - P]));
+        if (i < H - 1) rr = fsub(rr, fmul(G.wy[o], G.gy[o]));
+        return rr;
+    } else if (MODE == 3) {
+        return G.r[o];
+    } else if (MODE == 1) {
+        const float ax = lap_at(U, G.wIx, G.wIy, i, j, H, W, P);
+        const float val = fsub(G.b[o], ax);
+        G.r[o] = val;
+        acc[0] += isfinite(val) ? 0.0 : 1.0;
+        return val;
+    } else {
+        const float xn = fmaf(alpha, pk[o], U[o]);
+        const float rn = fmaf(-alpha, G.Ap[o], G.r[o]);
+        U[o] = xn;
+        G.r[o] = rn;
+        acc[0] += (double)rn * (double)rn;
+        acc[1] += isfinite(xn) ? 0.0 : 1.0;
+        return rn;
+    }
+}
+
+template <int MODE>
+__device__ __forceinline__ void rowfwd_finalize(InstState* st, const double (&acc)[2]) {
+    if (MODE == 1) {
+        // non-finite initial residual: CG returns x0 (utils_unwrap2d.py:1418-1419)
+        st->cg_active = acc[0] == 0.0 ? 1 : 0;
+    } else if (MODE == 2) {
+        const double rn = sqrt(acc[0]);
+        st->rnorm = rn;
+        if (acc[1] != 0.0 || !(rn >= (double)st->cg_tol) || !isfinite(rn)) st->cg_active = 0;
+    }
+}
+
+// Row-inverse modes:
+//  0 INITU u = nan_to_num(z) (utils_unwrap2d.py:1498-1502), sum of u * valid
+//  1 Z0    z = M^-1 r, rz = r.z                (utils_unwrap2d.py:1421-1428)
+//  2 Z     z = M^-1 r, beta from r.z          (utils_unwrap2d.py:1461-1472)
+//  3 COPY  z as computed (operator entry point)
+template <int MODE>
+__device__ __forceinline__ bool rowinv_gate(const InstState* s) {
+    if (MODE == 0 || MODE == 3) return true;
+    return s->irls_active != 0 && s->cg_active != 0;
+}
+
+template <int MODE>
+__device__ __forceinline__ void rowinv_store(const GridDev& G, int i, int j, float zv, double (&acc)[2]) {
+    const size_t o = (size_t)i * G.P + j;
+    if (MODE == 3) {
+        G.z[o] = zv;
+    } else if (MODE == 0) {
+        const float u = isfinite(zv) ? zv : 0.f;
+        acc[1] += isfinite(zv) ? 0.0 : 1.0;
+        G.U0[o] = u;
+        // (u * valid_float).sum(): an invalid pixel contributes u * 0
+        acc[0] += (double)(u * (G.valid[o] ? 1.f : 0.f));
+    } else {
+        G.z[o] = zv;
+        acc[0] += (double)G.r[o] * (double)zv;
+    }
+}
+
+template <int MODE>
+__device__ __forceinline__ void rowinv_finalize(InstState* st, const double (&acc)[2]) {
+    if (MODE == 0) {
+        if (acc[1] != 0.0) st->status |= 1;  // UNW_S_DCT_INIT_NONFINITE
+        st->mean = st->vcount > 0 ? acc[0] / st->vcount : 0.0;
+    } else if (MODE == 1) {
+        st->rz = acc[0];
+    } else if (MODE == 2) {
+        const double rzn = acc[0];
+        if (fabs(st->rz) < 1e-15) {
+            st->cg_active = 0;
+        } else {
+            double be = rzn / st->rz;
+            be = be < -1e6 ? -1e6 : (be > 1e6 ? 1e6 : be);
+            st->beta = (float)be;
+            st->rz = rzn;
+        }
+    }
+}
+
+// Column-pass spectral step for one frequency pair (k, H-k) of two columns
+// (ja, ja+1) whose DFT outputs are C = C_k and Cm = C_{H-k}: DCT-II extraction,
+// division by the Neumann-Laplacian eigenvalue (computed in float64 and rounded
+// once, as utils_unwrap2d.py:1284-1289 does), negation, DC term zeroed, then
+// the DCT-III pre-twiddle.  Returns conj(C'_k) ready for a forward FFT.
+__device__ __forceinline__ float2 col_spectral(float2 C, float2 Cm, int k, int km, float2 wk, float2 wm,
+                                               double ck, double cm, double ca, double cb, bool ja0, bool hasb,
+                                               float negs) {
+    const float2 Vak = make_float2(C.x + Cm.x, C.y - Cm.y);
+    const float2 Vbk = make_float2(C.y + Cm.y, Cm.x - C.x);
+    const float2 Vam = make_float2(Cm.x + C.x, Cm.y - C.y);
+    const float2 Vbm = make_float2(Cm.y + C.y, C.x - Cm.x);
+    float Xak = wk.x * Vak.x - wk.y * Vak.y, Xbk = wk.x * Vbk.x - wk.y * Vbk.y;
+    float Xam = wm.x * Vam.x - wm.y * Vam.y, Xbm = wm.x * Vbm.x - wm.y * Vbm.y;
+    const float lak = (float)(2.0 * ck + 2.0 * ca - 4.0), lbk = (float)(2.0 * ck + 2.0 * cb - 4.0);
+    const float lam = (float)(2.0 * cm + 2.0 * ca - 4.0), lbm = (float)(2.0 * cm + 2.0 * cb - 4.0);
+    Xak = (k == 0 && ja0) ? 0.f : fdiv(Xak, lak) * negs;
+    Xam = (km == 0 && ja0) ? 0.f : fdiv(Xam, lam) * negs;
+    Xbk = hasb ? fdiv(Xbk, lbk) * negs : 0.f;
+    Xbm = hasb ? fdiv(Xbm, lbm) * negs : 0.f;
+    const float mak = k == 0 ? 0.f : Xam, mbk = k == 0 ? 0.f : Xbm;
+    const float2 Pak = cmul(cconj(wk), make_float2(Xak, -mak));
+    const float2 Pbk = cmul(cconj(wk), make_float2(Xbk, -mbk));
+    return cconj(make_float2(Pak.x - Pbk.y, Pak.y + Pbk.x));
+}

@@ -18,6 +18,7 @@
 // accumulate in float64.
 #include <climits>
 #include "unw_fft.cuh"
+#include "unw_rowops.cuh"
 #include "unw_kernels.h"
 
 // ============================================================ tables
@@ -137,34 +138,9 @@ __global__ void k_setup(const GridDev* __restrict__ grids, const int* __restrict
     }
 }
 
-// ============================================================ Laplacian helpers
-// A x at (i, j): -div(w grad x) in the reference's op order (utils_unwrap2d.py:1367-1388):
-// res = 0; res -= dx[j-1]; res += dx[j]; res -= dy[i-1]; res += dy[i]; Ax = -res.
-__device__ __forceinline__ float lap_at(const float* __restrict__ x, const float* __restrict__ wx,
-                                        const float* __restrict__ wy, int i, int j, int H, int W, int P) {
-    const size_t o = (size_t)i * P + j;
-    const float xc = x[o];
-    float res = 0.f;
-    if (j > 0) res = fsub(res, fmul(fsub(xc, x[o - 1]), wx[o - 1]));
-    if (j < W - 1) res = fadd(res, fmul(fsub(x[o + 1], xc), wx[o]));
-    if (i > 0) res = fsub(res, fmul(fsub(xc, x[o - P]), wy[o - P]));
-    if (i < H - 1) res = fadd(res, fmul(fsub(x[o + P], xc), wy[o]));
-    return -res;
-}
-
 // ============================================================ row forward pass
-// Row DCT-II of rows (i0, i0+1) of a source computed on the fly.
-// MODE 0 (RHO):  rho = -div(w g), the DCT initial solve (utils_unwrap2d.py:1478-1483)
-// MODE 1 (R0):   r = b - A x0, PCG start (utils_unwrap2d.py:1413-1419)
-// MODE 2 (UPD):  x += alpha p; r -= alpha Ap (utils_unwrap2d.py:1445-1459)
-// Output T[i][k] = 2 * DCT-II(row i)[k] / 2 (unnormalised, no 1/2 factor).
-template <int MODE>
-__device__ __forceinline__ bool rowfwd_gate(const InstState* s) {
-    if (MODE == 0 || MODE == 3) return true;
-    if (MODE == 1) return s->irls_active != 0;
-    return s->irls_active != 0 && s->cg_active != 0;
-}
-
+// Generic lengths: row DCT-II of rows (i0, i0+1) of a source computed on the
+// fly (modes in unw_rowops.cuh).  Output T[i][k] = DCT-II(row i)[k] (no 1/2).
 template <int T, int EMAX, int MODE>
 __global__ void __launch_bounds__(T) k_row_fwd(const GridDev* __restrict__ grids,
                                                const int* __restrict__ starts, int n, int it,
@@ -185,38 +161,8 @@ __global__ void __launch_bounds__(T) k_row_fwd(const GridDev* __restrict__ grids
     const float* pk = (MODE == 2) ? ((cgk & 1) ? G.p1 : G.p0) : nullptr;
     const float alpha = (MODE == 2) ? st->alpha : 0.f;
     for (int j = threadIdx.x; j < W; j += T) {
-        float a = 0.f, b = 0.f;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int i = i0 + h;
-            if (h == 1 && !has1) break;
-            const size_t o = (size_t)i * P + j;
-            float val;
-            if (MODE == 0) {
-                float rr = 0.f;
-                if (j > 0) rr = fadd(rr, fmul(G.wx[o - 1], G.gx[o - 1]));
-                if (j < W - 1) rr = fsub(rr, fmul(G.wx[o], G.gx[o]));
-                if (i > 0) rr = fadd(rr, fmul(G.wy[o - P], G.gy[o - P]));
-                if (i < H - 1) rr = fsub(rr, fmul(G.wy[o], G.gy[o]));
-                val = rr;
-            } else if (MODE == 3) {
-                val = G.r[o];
-            } else if (MODE == 1) {
-                const float ax = lap_at(U, G.wIx, G.wIy, i, j, H, W, P);
-                val = fsub(G.b[o], ax);
-                G.r[o] = val;
-                acc[0] += isfinite(val) ? 0.0 : 1.0;
-            } else {
-                const float xn = fmaf(alpha, pk[o], U[o]);
-                const float rn = fmaf(-alpha, G.Ap[o], G.r[o]);
-                U[o] = xn;
-                G.r[o] = rn;
-                acc[0] += (double)rn * (double)rn;
-                acc[1] += isfinite(xn) ? 0.0 : 1.0;
-                val = rn;
-            }
-            if (h == 0) a = val; else b = val;
-        }
+        const float a = rowfwd_value<MODE>(G, U, pk, alpha, i0, j, acc);
+        const float b = has1 ? rowfwd_value<MODE>(G, U, pk, alpha, i1, j, acc) : 0.f;
         sm[mk_perm(j, W)] = make_float2(a, b);
     }
     __syncthreads();
@@ -235,16 +181,7 @@ __global__ void __launch_bounds__(T) k_row_fwd(const GridDev* __restrict__ grids
     if (MODE == 0 || MODE == 3) return;
     if (arrive<2>(G, local, nct, acc, red)) {
         finish_sum<2>(G, nct, acc, red);
-        if (threadIdx.x == 0) {
-            if (MODE == 1) {
-                // non-finite initial residual: CG returns x0 (utils_unwrap2d.py:1418-1419)
-                st->cg_active = acc[0] == 0.0 ? 1 : 0;
-            } else {
-                const double rn = sqrt(acc[0]);
-                st->rnorm = rn;
-                if (acc[1] != 0.0 || !(rn >= (double)st->cg_tol) || !isfinite(rn)) st->cg_active = 0;
-            }
-        }
+        if (threadIdx.x == 0) rowfwd_finalize<MODE>(st, acc);
     }
 }
 
@@ -286,34 +223,13 @@ __global__ void __launch_bounds__(T) k_col(const GridDev* __restrict__ grids,
         if (k > km) continue;
         float2* base = sm + s * sd;
         const float2 C = base[k], Cm = base[km];
-        const int ja = c0 + 2 * s, jb = ja + 1;
-        // DCT-II of the two columns at frequencies k and km
+        const int ja = c0 + 2 * s;
+        const bool hasb = ja + 1 < W;
+        const double ca = cW[ja], cb = hasb ? cW[ja + 1] : 1.0;
         const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
-        const float2 Vak = make_float2(C.x + Cm.x, C.y - Cm.y);
-        const float2 Vbk = make_float2(C.y + Cm.y, Cm.x - C.x);
-        const float2 Vam = make_float2(Cm.x + C.x, Cm.y - C.y);
-        const float2 Vbm = make_float2(Cm.y + C.y, C.x - Cm.x);
-        float Xak = wk.x * Vak.x - wk.y * Vak.y, Xbk = wk.x * Vbk.x - wk.y * Vbk.y;
-        float Xam = wm.x * Vam.x - wm.y * Vam.y, Xbm = wm.x * Vbm.x - wm.y * Vbm.y;
-        // divide by the Neumann-Laplacian eigenvalue, negate, zero the DC term
-        const double ck = cH[k], cm = cH[km];
-        const double ca = cW[ja], cb = jb < W ? cW[jb] : 1.0;
-        const float lak = (float)(2.0 * ck + 2.0 * ca - 4.0), lbk = (float)(2.0 * ck + 2.0 * cb - 4.0);
-        const float lam = (float)(2.0 * cm + 2.0 * ca - 4.0), lbm = (float)(2.0 * cm + 2.0 * cb - 4.0);
-        Xak = (k == 0 && ja == 0) ? 0.f : fdiv(Xak, lak) * negs;
-        Xam = (km == 0 && ja == 0) ? 0.f : fdiv(Xam, lam) * negs;
-        Xbk = jb < W ? fdiv(Xbk, lbk) * negs : 0.f;
-        Xbm = jb < W ? fdiv(Xbm, lbm) * negs : 0.f;
-        // DCT-III pre-twiddle: V'_k = conj(w_k) (Y_k - i Y_{H-k}), Y_H = 0; store conj(C')
-        const float mak = k == 0 ? 0.f : Xam, mbk = k == 0 ? 0.f : Xbm;
-        const float2 Pak = cmul(cconj(wk), make_float2(Xak, -mak));
-        const float2 Pbk = cmul(cconj(wk), make_float2(Xbk, -mbk));
-        base[k] = cconj(make_float2(Pak.x - Pbk.y, Pak.y + Pbk.x));
-        if (km != k) {
-            const float2 Pam = cmul(cconj(wm), make_float2(Xam, -Xak));
-            const float2 Pbm = cmul(cconj(wm), make_float2(Xbm, -Xbk));
-            base[km] = cconj(make_float2(Pam.x - Pbm.y, Pam.y + Pbm.x));
-        }
+        const float2 ok = col_spectral(C, Cm, k, km, wk, wm, cH[k], cH[km], ca, cb, ja == 0, hasb, negs);
+        if (km != k) base[km] = col_spectral(Cm, C, km, k, wm, wk, cH[km], cH[k], ca, cb, ja == 0, hasb, negs);
+        base[k] = ok;
     }
     __syncthreads();
     dft_n<T, EMAX>(sm, nseq, PC);
@@ -327,16 +243,8 @@ __global__ void __launch_bounds__(T) k_col(const GridDev* __restrict__ grids,
 }
 
 // ============================================================ row inverse pass
-// Row DCT-III of rows (i0, i0+1) of T, with the epilogue:
-// MODE 0 (INITU): u = nan_to_num(z) (utils_unwrap2d.py:1498-1502), sum over valid pixels
-// MODE 1 (Z0):    z = M^-1 r, rz = r.z                (utils_unwrap2d.py:1421-1428)
-// MODE 2 (Z):     z = M^-1 r, beta from r.z          (utils_unwrap2d.py:1461-1472)
-template <int MODE>
-__device__ __forceinline__ bool rowinv_gate(const InstState* s) {
-    if (MODE == 0 || MODE == 3) return true;
-    return s->irls_active != 0 && s->cg_active != 0;
-}
-
+// Generic lengths: row DCT-III of rows (i0, i0+1) of T with the epilogue of
+// MODE (unw_rowops.cuh).
 template <int T, int EMAX, int MODE>
 __global__ void __launch_bounds__(T) k_row_inv(const GridDev* __restrict__ grids,
                                                const int* __restrict__ starts, int n) {
@@ -380,59 +288,48 @@ __global__ void __launch_bounds__(T) k_row_inv(const GridDev* __restrict__ grids
     double acc[2] = {0.0, 0.0};
     for (int j = threadIdx.x; j < W; j += T) {
         const float2 v = sm[mk_perm(j, W)];
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            if (h == 1 && !has1) break;
-            const int i = i0 + h;
-            const size_t o = (size_t)i * P + j;
-            const float zv = h == 0 ? v.x : -v.y;
-            if (MODE == 3) {
-                G.z[o] = zv;
-            } else if (MODE == 0) {
-                const float u = isfinite(zv) ? zv : 0.f;
-                acc[1] += isfinite(zv) ? 0.0 : 1.0;
-                G.U0[o] = u;
-                // (u * valid_float).sum(): an invalid pixel contributes u * 0
-                acc[0] += (double)(u * (G.valid[o] ? 1.f : 0.f));
-            } else {
-                G.z[o] = zv;
-                acc[0] += (double)G.r[o] * (double)zv;
-            }
-        }
+        rowinv_store<MODE>(G, i0, j, v.x, acc);
+        if (has1) rowinv_store<MODE>(G, i1, j, -v.y, acc);
     }
     if (MODE == 3) return;
     if (arrive<2>(G, local, nct, acc, red)) {
         finish_sum<2>(G, nct, acc, red);
-        if (threadIdx.x == 0) {
-            if (MODE == 0) {
-                if (acc[1] != 0.0) st->status |= 1;  // UNW_S_DCT_INIT_NONFINITE
-                st->mean = st->vcount > 0 ? acc[0] / st->vcount : 0.0;
-            } else if (MODE == 1) {
-                st->rz = acc[0];
-            } else {
-                const double rzn = acc[0];
-                if (fabs(st->rz) < 1e-15) {
-                    st->cg_active = 0;
-                } else {
-                    double be = rzn / st->rz;
-                    be = be < -1e6 ? -1e6 : (be > 1e6 ? 1e6 : be);
-                    st->beta = (float)be;
-                    st->rz = rzn;
-                }
-            }
-        }
+        if (threadIdx.x == 0) rowinv_finalize<MODE>(st, acc);
     }
 }
 
 // ============================================================ stencil kernels
-// KS_STEN shape: a CTA covers 256 columns x sten_rows rows.
-// matvec: p = z + beta p_old (p = z on the first PCG iteration), Ap = A p,
-// pAp = p.Ap (utils_unwrap2d.py:1430-1443, :1471).
-__device__ __forceinline__ float pnew_at(const float* __restrict__ z, const float* __restrict__ po,
-                                         size_t o, bool first, float beta) {
+// KS_STEN shape: a CTA is 8 warps; warp w of tile (tx, ty) covers columns
+// [128 tx, 128 tx + 128) (4 per lane) and rows [(8 ty + w) R, (8 ty + w + 1) R),
+// R = sten_rows, marching down the rows with the row above and below in registers.
+struct F4 {
+    float v[4];
+};
+__device__ __forceinline__ F4 ld4(const float* __restrict__ a, size_t o) {
+    const float4 x = *reinterpret_cast<const float4*>(a + o);
+    return F4{{x.x, x.y, x.z, x.w}};
+}
+__device__ __forceinline__ void st4(float* __restrict__ a, size_t o, const F4& x) {
+    *reinterpret_cast<float4*>(a + o) = make_float4(x.v[0], x.v[1], x.v[2], x.v[3]);
+}
+
+// p = z + beta p_old (reference: p.mul_(beta).add_(z)), p = z on the first PCG step
+__device__ __forceinline__ F4 pnew4(const float* __restrict__ z, const float* __restrict__ po, size_t o,
+                                    bool first, float beta) {
+    F4 r = ld4(z, o);
+    if (!first) {
+        const F4 q = ld4(po, o);
+#pragma unroll
+        for (int c = 0; c < 4; c++) r.v[c] = fadd(fmul(q.v[c], beta), r.v[c]);
+    }
+    return r;
+}
+__device__ __forceinline__ float pnew1(const float* __restrict__ z, const float* __restrict__ po, size_t o,
+                                       bool first, float beta) {
     return first ? z[o] : fadd(fmul(po[o], beta), z[o]);
 }
 
+// matvec: p = z + beta p_old, Ap = A p, pAp = p.Ap (utils_unwrap2d.py:1430-1443, :1471)
 __global__ void __launch_bounds__(256) k_matvec(const GridDev* __restrict__ grids,
                                                 const int* __restrict__ starts, int n, int k) {
     __shared__ double red[32 * 1];
@@ -443,28 +340,66 @@ __global__ void __launch_bounds__(256) k_matvec(const GridDev* __restrict__ grid
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tx = local % G.sten_tiles_x, ty = local / G.sten_tiles_x;
-    const int j = tx * 256 + threadIdx.x;
-    const int ib = ty * G.sten_rows, ie = min(H, ib + G.sten_rows);
+    const int j0 = tx * 128 + lane * 4;
+    const int ib = (ty * 8 + warp) * G.sten_rows, ie = min(H, ib + G.sten_rows);
     const bool first = st->pfirst != 0;
     const float beta = st->beta;
     const float* __restrict__ z = G.z;
     const float* __restrict__ po = (k & 1) ? G.p0 : G.p1;
     float* __restrict__ pn = (k & 1) ? G.p1 : G.p0;
+    const float* __restrict__ wIx = G.wIx;
+    const float* __restrict__ wIy = G.wIy;
     double acc[1] = {0.0};
-    if (j < W) {
-        for (int i = ib; i < ie; i++) {
-            const size_t o = (size_t)i * P + j;
-            const float pc = pnew_at(z, po, o, first, beta);
-            float res = 0.f;
-            if (j > 0) res = fsub(res, fmul(fsub(pc, pnew_at(z, po, o - 1, first, beta)), G.wIx[o - 1]));
-            if (j < W - 1) res = fadd(res, fmul(fsub(pnew_at(z, po, o + 1, first, beta), pc), G.wIx[o]));
-            if (i > 0) res = fsub(res, fmul(fsub(pc, pnew_at(z, po, o - P, first, beta)), G.wIy[o - P]));
-            if (i < H - 1) res = fadd(res, fmul(fsub(pnew_at(z, po, o + P, first, beta), pc), G.wIy[o]));
-            const float ap = -res;
-            pn[o] = pc;
-            G.Ap[o] = ap;
-            acc[0] += (double)pc * (double)ap;
+    // lanes past the last column load nothing (j0 < W implies j0 + 3 < P)
+    const bool lane_on = j0 < W;
+    if (ib < H) {
+        F4 up{}, wyu{}, cur{}, dn{};
+        size_t o = (size_t)ib * P + j0;
+        if (lane_on) cur = pnew4(z, po, o, first, beta);
+        if (ib > 0 && lane_on) {
+            up = pnew4(z, po, o - P, first, beta);
+            wyu = ld4(wIy, o - P);
+        }
+        for (int i = ib; i < ie; i++, o += P) {
+            F4 wx{}, wy{};
+            if (lane_on) {
+                if (i < H - 1) dn = pnew4(z, po, o + P, first, beta);
+                wx = ld4(wIx, o);
+                wy = ld4(wIy, o);
+            }
+            float pl = __shfl_up_sync(0xffffffffu, cur.v[3], 1);
+            float wl = __shfl_up_sync(0xffffffffu, wx.v[3], 1);
+            float pr = __shfl_down_sync(0xffffffffu, cur.v[0], 1);
+            if (lane == 0 && j0 > 0) {
+                pl = pnew1(z, po, o - 1, first, beta);
+                wl = wIx[o - 1];
+            }
+            if (lane == 31 && j0 + 4 < W) pr = pnew1(z, po, o + 4, first, beta);
+            F4 ap;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int j = j0 + c;
+                const float pc = cur.v[c];
+                const float pleft = c == 0 ? pl : cur.v[c - 1];
+                const float pright = c == 3 ? pr : cur.v[c + 1];
+                const float wleft = c == 0 ? wl : wx.v[c - 1];
+                float res = 0.f;
+                if (j > 0) res = fsub(res, fmul(fsub(pc, pleft), wleft));
+                if (j < W - 1) res = fadd(res, fmul(fsub(pright, pc), wx.v[c]));
+                if (i > 0) res = fsub(res, fmul(fsub(pc, up.v[c]), wyu.v[c]));
+                if (i < H - 1) res = fadd(res, fmul(fsub(dn.v[c], pc), wy.v[c]));
+                ap.v[c] = -res;
+                if (j < W) acc[0] += (double)pc * (double)ap.v[c];
+            }
+            if (lane_on) {
+                st4(pn, o, cur);
+                st4(G.Ap, o, ap);
+            }
+            up = cur;
+            cur = dn;
+            wyu = wy;
         }
     }
     if (arrive<1>(G, local, nct, acc, red)) {
@@ -488,6 +423,10 @@ __global__ void __launch_bounds__(256) k_matvec(const GridDev* __restrict__ grid
 // IRLS head (utils_unwrap2d.py:1536-1581): recentre, residual gradients,
 // best-iterate test, IRLS weights and right-hand side.  Reads U_cur, writes
 // the recentred iterate to U_nxt (U_cur keeps u_prev for the convergence test).
+__device__ __forceinline__ float irls_w(float w, float r, float eps2) {
+    return clampf_nan(fdiv(w, __fsqrt_rn(fadd(fmul(r, r), eps2))), 1e-6f, 1e6f);
+}
+
 __global__ void __launch_bounds__(256) k_head(const GridDev* __restrict__ grids,
                                               const int* __restrict__ starts, int n, int it) {
     __shared__ double red[32 * 2];
@@ -498,41 +437,40 @@ __global__ void __launch_bounds__(256) k_head(const GridDev* __restrict__ grids,
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tx = local % G.sten_tiles_x, ty = local / G.sten_tiles_x;
-    const int j = tx * 256 + threadIdx.x;
-    const int ib = ty * G.sten_rows, ie = min(H, ib + G.sten_rows);
+    const int j0 = tx * 128 + lane * 4;
+    const int ib = (ty * 8 + warp) * G.sten_rows, ie = min(H, ib + G.sten_rows);
     const float m = st->vcount > 0 ? (float)st->mean : 0.f;
     const float eps2 = st->eps2;
     const float* __restrict__ uc = (it & 1) ? G.U1 : G.U0;
     float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
     double acc[2] = {0.0, 0.0};
-    if (j < W) {
-        for (int i = ib; i < ie; i++) {
+    for (int i = ib; i < ie; i++) {
+        for (int c = 0; c < 4; c++) {
+            const int j = j0 + c;
+            if (j >= W) break;
             const size_t o = (size_t)i * P + j;
-            const float c = fsub(uc[o], m);
+            const float cv = fsub(uc[o], m);
             // residual gradients r = grad(u) - g (last column/row: 0 - g)
-            const float rx = (j < W - 1) ? fsub(fsub(fsub(uc[o + 1], m), c), G.gx[o]) : fsub(0.f, G.gx[o]);
-            const float ry = (i < H - 1) ? fsub(fsub(fsub(uc[o + P], m), c), G.gy[o]) : fsub(0.f, G.gy[o]);
+            const float rx = (j < W - 1) ? fsub(fsub(fsub(uc[o + 1], m), cv), G.gx[o]) : fsub(0.f, G.gx[o]);
+            const float ry = (i < H - 1) ? fsub(fsub(fsub(uc[o + P], m), cv), G.gy[o]) : fsub(0.f, G.gy[o]);
             acc[0] += (double)fmul(rx, rx) + (double)fmul(ry, ry);
-            acc[1] += isfinite(c) ? 0.0 : 1.0;
-            const float wix = clampf_nan(fdiv(G.wx[o], __fsqrt_rn(fadd(fmul(rx, rx), eps2))), 1e-6f, 1e6f);
-            const float wiy = clampf_nan(fdiv(G.wy[o], __fsqrt_rn(fadd(fmul(ry, ry), eps2))), 1e-6f, 1e6f);
+            acc[1] += isfinite(cv) ? 0.0 : 1.0;
+            const float wix = irls_w(G.wx[o], rx, eps2);
+            const float wiy = irls_w(G.wy[o], ry, eps2);
             float bv = 0.f;
             if (j > 0) {
-                const float l = fsub(uc[o - 1], m);
-                const float rxl = fsub(fsub(c, l), G.gx[o - 1]);
-                const float wl = clampf_nan(fdiv(G.wx[o - 1], __fsqrt_rn(fadd(fmul(rxl, rxl), eps2))), 1e-6f, 1e6f);
-                bv = fadd(bv, fmul(wl, G.gx[o - 1]));
+                const float rxl = fsub(fsub(cv, fsub(uc[o - 1], m)), G.gx[o - 1]);
+                bv = fadd(bv, fmul(irls_w(G.wx[o - 1], rxl, eps2), G.gx[o - 1]));
             }
             if (j < W - 1) bv = fsub(bv, fmul(wix, G.gx[o]));
             if (i > 0) {
-                const float u = fsub(uc[o - P], m);
-                const float ryu = fsub(fsub(c, u), G.gy[o - P]);
-                const float wu = clampf_nan(fdiv(G.wy[o - P], __fsqrt_rn(fadd(fmul(ryu, ryu), eps2))), 1e-6f, 1e6f);
-                bv = fadd(bv, fmul(wu, G.gy[o - P]));
+                const float ryu = fsub(fsub(cv, fsub(uc[o - P], m)), G.gy[o - P]);
+                bv = fadd(bv, fmul(irls_w(G.wy[o - P], ryu, eps2), G.gy[o - P]));
             }
             if (i < H - 1) bv = fsub(bv, fmul(wiy, G.gy[o]));
-            un[o] = c;
+            un[o] = cv;
             G.wIx[o] = wix;
             G.wIy[o] = wiy;
             G.b[o] = bv;

@@ -138,7 +138,8 @@ def ref_setup(phase, weight):
 
 # ------------------------------------------------------------------ operator kernels
 SHAPES = [(64, 64), (37, 50), (128, 96), (17, 257), (1, 7), (5, 1), (3, 5), (1, 1), (200, 131),
-          (1024, 1024), (2600, 4001), (4096, 4096)]
+          (1024, 1024), (2600, 4001), (4096, 4096), (256, 512), (512, 256), (2048, 1000), (1000, 2048),
+          (4096, 333), (6, 16384), (8192, 10)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
