@@ -1,21 +1,67 @@
-// DCT passes for power-of-two grid dimensions on the register-resident FFT.
+// DCT passes for power-of-two grid dimensions on the register/shared-memory
+// radix-16 FFT (unw_regfft.cuh).
 //
 // Row passes: one CTA of N/16 threads per pair of rows (two real rows are the
-// real and imaginary parts of one complex length-N sequence).  Thread t
-// handles FFT positions m = t + (N/16) q, whose source column is Makhoul's
-// n(m) = 2m (m < N/2) or 2N-1-2m, so the even/odd reordering costs nothing:
-// it is just the address each thread loads (and, for the inverse, stores).
+// real and imaginary parts of one complex length-N sequence).  Global I/O is
+// coalesced float4; Makhoul's even/odd reordering (x_n sits at FFT position
+// n/2 for even n, N-1-(n-1)/2 for odd n) is a scatter into / gather from
+// shared memory, so it costs no extra pass over HBM.
 //
-// Column pass: NSEQ column pairs per CTA; forward FFT, spectral step
-// (DCT-II extraction, -1/lambda scaling, DCT-III pre-twiddle) done in
-// registers for k with C_{N-k} read from shared memory, inverse FFT, store.
+// Column pass: NSEQ column pairs per CTA; forward FFT, spectral step on
+// frequency pairs (k, N-k) in shared memory (DCT-II extraction, -1/lambda
+// scaling, DCT-III pre-twiddle), inverse FFT, store.
 #include "unw_regfft.cuh"
 #include "unw_rowops.cuh"
 #include "unw_kernels.h"
 
+template <int T>
+constexpr int min_blocks() { return T >= 1024 ? 1 : (1024 / T > 16 ? 16 : 1024 / T); }
+
+__device__ __forceinline__ int mk_pos(int n, int N) { return (n & 1) ? N - 1 - (n >> 1) : (n >> 1); }
+
+__device__ __forceinline__ float4 ld4f(const float* __restrict__ a, size_t o) {
+    return *reinterpret_cast<const float4*>(a + o);
+}
+__device__ __forceinline__ void st4f(float* __restrict__ a, size_t o, float4 v) {
+    *reinterpret_cast<float4*>(a + o) = v;
+}
+__device__ __forceinline__ float f4get(const float4& v, int c) {
+    return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
+}
+
+// Four consecutive source values of row i (columns j..j+3) of the row-forward pass.
+template <int MODE>
+__device__ __forceinline__ float4 rowf_vals4(const GridDev& G, float* __restrict__ U, const float* __restrict__ pk,
+                                             float alpha, int i, int j, double (&acc)[2]) {
+    const size_t o = (size_t)i * G.P + j;
+    if (MODE == 2) {
+        const float4 x = ld4f(U, o), p = ld4f(pk, o), r = ld4f(G.r, o), ap = ld4f(G.Ap, o);
+        float4 xn, rn;
+        xn.x = fmaf(alpha, p.x, x.x); xn.y = fmaf(alpha, p.y, x.y);
+        xn.z = fmaf(alpha, p.z, x.z); xn.w = fmaf(alpha, p.w, x.w);
+        rn.x = fmaf(-alpha, ap.x, r.x); rn.y = fmaf(-alpha, ap.y, r.y);
+        rn.z = fmaf(-alpha, ap.z, r.z); rn.w = fmaf(-alpha, ap.w, r.w);
+        st4f(U, o, xn);
+        st4f(G.r, o, rn);
+        acc[0] += (double)rn.x * rn.x + (double)rn.y * rn.y + (double)rn.z * rn.z + (double)rn.w * rn.w;
+        acc[1] += (isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z) && isfinite(xn.w)) ? 0.0 : 1.0;
+        return rn;
+    } else if (MODE == 3) {
+        return ld4f(G.r, o);
+    } else {
+        float4 v;
+        v.x = rowfwd_value<MODE>(G, U, pk, alpha, i, j, acc);
+        v.y = rowfwd_value<MODE>(G, U, pk, alpha, i, j + 1, acc);
+        v.z = rowfwd_value<MODE>(G, U, pk, alpha, i, j + 2, acc);
+        v.w = rowfwd_value<MODE>(G, U, pk, alpha, i, j + 3, acc);
+        return v;
+    }
+}
+
 template <int N, int MODE>
-__global__ void __launch_bounds__(N / 16) k_rowf_p2(const GridDev* __restrict__ grids,
-                                                    const int* __restrict__ starts, int n, int it, int cgk) {
+__global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowf_p2(const GridDev* __restrict__ grids,
+                                                                         const int* __restrict__ starts, int n,
+                                                                         int it, int cgk) {
     constexpr int T = N / 16;
     extern __shared__ float2 sm[];
     __shared__ double red[32 * 2];
@@ -33,31 +79,34 @@ __global__ void __launch_bounds__(N / 16) k_rowf_p2(const GridDev* __restrict__ 
     const float* pk = (MODE == 2) ? ((cgk & 1) ? G.p1 : G.p0) : nullptr;
     const float alpha = (MODE == 2) ? st->alpha : 0.f;
     double acc[2] = {0.0, 0.0};
-    float2 v[16];
+    for (int c4 = t; c4 < N / 4; c4 += T) {
+        const int j = 4 * c4;
+        const float4 a = rowf_vals4<MODE>(G, U, pk, alpha, i0, j, acc);
+        const float4 b = has1 ? rowf_vals4<MODE>(G, U, pk, alpha, i1, j, acc) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-        const int j = mk_src<N>(t + T * q);
-        const float a = rowfwd_value<MODE>(G, U, pk, alpha, i0, j, acc);
-        const float b = has1 ? rowfwd_value<MODE>(G, U, pk, alpha, i1, j, acc) : 0.f;
-        v[q] = make_float2(a, b);
+        for (int c = 0; c < 4; c++) sm[pad16(mk_pos(j + c, N))] = make_float2(f4get(a, c), f4get(b, c));
     }
-    reg_fft<N>(v, sm, t, G.prow.fft.tw);
-#pragma unroll
-    for (int q = 0; q < 16; q++) sm[pad16(t + T * q)] = v[q];
     __syncthreads();
+    smem_fft<N>(sm, t, G.prow.fft.tw);
+    // two real rows from one complex DFT, then X_k = Re(exp(-i pi k/2N) V_k)
     const float2* __restrict__ dw = G.prow.dctw;
     float* __restrict__ Ta = G.T + (size_t)i0 * P;
     float* __restrict__ Tb = G.T + (size_t)i1 * P;
+    for (int c4 = t; c4 < N / 4; c4 += T) {
+        float xa[4], xb[4];
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-        const int k = t + T * q;
-        const float2 C = v[q];
-        const float2 Cm = sm[pad16((N - k) & (N - 1))];
-        const float2 w = __ldg(&dw[k]);
-        const float2 Va = make_float2(C.x + Cm.x, C.y - Cm.y);
-        const float2 Vb = make_float2(C.y + Cm.y, Cm.x - C.x);
-        Ta[k] = w.x * Va.x - w.y * Va.y;
-        if (has1) Tb[k] = w.x * Vb.x - w.y * Vb.y;
+        for (int c = 0; c < 4; c++) {
+            const int k = 4 * c4 + c;
+            const float2 C = sm[pad16(k)];
+            const float2 Cm = sm[pad16((N - k) & (N - 1))];
+            const float2 w = __ldg(&dw[k]);
+            const float2 Va = make_float2(C.x + Cm.x, C.y - Cm.y);
+            const float2 Vb = make_float2(C.y + Cm.y, Cm.x - C.x);
+            xa[c] = w.x * Va.x - w.y * Va.y;
+            xb[c] = w.x * Vb.x - w.y * Vb.y;
+        }
+        st4f(Ta, 4 * c4, make_float4(xa[0], xa[1], xa[2], xa[3]));
+        if (has1) st4f(Tb, 4 * c4, make_float4(xb[0], xb[1], xb[2], xb[3]));
     }
     if (MODE == 0 || MODE == 3) return;
     if (arrive<2>(G, local, nct, acc, red)) {
@@ -66,9 +115,31 @@ __global__ void __launch_bounds__(N / 16) k_rowf_p2(const GridDev* __restrict__ 
     }
 }
 
+// Epilogue of the row-inverse pass for columns j..j+3 of row i.
+template <int MODE>
+__device__ __forceinline__ void rowi_store4(const GridDev& G, int i, int j, float4 z, double (&acc)[2]) {
+    const size_t o = (size_t)i * G.P + j;
+    if (MODE == 3) {
+        st4f(G.z, o, z);
+    } else if (MODE == 0) {
+        float4 u;
+        u.x = isfinite(z.x) ? z.x : 0.f; u.y = isfinite(z.y) ? z.y : 0.f;
+        u.z = isfinite(z.z) ? z.z : 0.f; u.w = isfinite(z.w) ? z.w : 0.f;
+        acc[1] += (isfinite(z.x) && isfinite(z.y) && isfinite(z.z) && isfinite(z.w)) ? 0.0 : 1.0;
+        st4f(G.U0, o, u);
+        const uchar4 v = *reinterpret_cast<const uchar4*>(G.valid + o);
+        acc[0] += (double)(u.x * (v.x ? 1.f : 0.f)) + (double)(u.y * (v.y ? 1.f : 0.f)) +
+                  (double)(u.z * (v.z ? 1.f : 0.f)) + (double)(u.w * (v.w ? 1.f : 0.f));
+    } else {
+        st4f(G.z, o, z);
+        const float4 r = ld4f(G.r, o);
+        acc[0] += (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z + (double)r.w * z.w;
+    }
+}
+
 template <int N, int MODE>
-__global__ void __launch_bounds__(N / 16) k_rowi_p2(const GridDev* __restrict__ grids,
-                                                    const int* __restrict__ starts, int n) {
+__global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const GridDev* __restrict__ grids,
+                                                                         const int* __restrict__ starts, int n) {
     constexpr int T = N / 16;
     extern __shared__ float2 sm[];
     __shared__ double red[32 * 2];
@@ -85,25 +156,35 @@ __global__ void __launch_bounds__(N / 16) k_rowi_p2(const GridDev* __restrict__ 
     const float* __restrict__ Ta = G.T + (size_t)i0 * P;
     const float* __restrict__ Tb = G.T + (size_t)i1 * P;
     const float2* __restrict__ dw = G.prow.dctw;
-    float2 v[16];
+    // DCT-III pre-twiddle: V'_k = conj(w_k) (Y_k - i Y_{N-k}), Y_N = 0; store conj(C')
+    for (int c4 = t; c4 < N / 4; c4 += T) {
+        const float4 ya = ld4f(Ta, 4 * c4);
+        const float4 yb = has1 ? ld4f(Tb, 4 * c4) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-        const int k = t + T * q;
-        const int km = (N - k) & (N - 1);
-        const float yak = Ta[k], ybk = has1 ? Tb[k] : 0.f;
-        const float yam = k ? Ta[km] : 0.f, ybm = (k && has1) ? Tb[km] : 0.f;
-        const float2 wc = cconj(__ldg(&dw[k]));
-        const float2 Pa = cmul(wc, make_float2(yak, -yam));
-        const float2 Pb = cmul(wc, make_float2(ybk, -ybm));
-        v[q] = cconj(make_float2(Pa.x - Pb.y, Pa.y + Pb.x));
+        for (int c = 0; c < 4; c++) {
+            const int k = 4 * c4 + c;
+            const int km = (N - k) & (N - 1);
+            const float yam = k ? Ta[km] : 0.f, ybm = (k && has1) ? Tb[km] : 0.f;
+            const float2 wc = cconj(__ldg(&dw[k]));
+            const float2 Pa = cmul(wc, make_float2(f4get(ya, c), -yam));
+            const float2 Pb = cmul(wc, make_float2(f4get(yb, c), -ybm));
+            sm[pad16(k)] = cconj(make_float2(Pa.x - Pb.y, Pa.y + Pb.x));
+        }
     }
-    reg_fft<N>(v, sm, t, G.prow.fft.tw);
+    __syncthreads();
+    smem_fft<N>(sm, t, G.prow.fft.tw);
     double acc[2] = {0.0, 0.0};
+    for (int c4 = t; c4 < N / 4; c4 += T) {
+        const int j = 4 * c4;
+        float za[4], zb[4];
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-        const int j = mk_src<N>(t + T * q);
-        rowinv_store<MODE>(G, i0, j, v[q].x, acc);
-        if (has1) rowinv_store<MODE>(G, i1, j, -v[q].y, acc);
+        for (int c = 0; c < 4; c++) {
+            const float2 v = sm[pad16(mk_pos(j + c, N))];
+            za[c] = v.x;
+            zb[c] = -v.y;
+        }
+        rowi_store4<MODE>(G, i0, j, make_float4(za[0], za[1], za[2], za[3]), acc);
+        if (has1) rowi_store4<MODE>(G, i1, j, make_float4(zb[0], zb[1], zb[2], zb[3]), acc);
     }
     if (MODE == 3) return;
     if (arrive<2>(G, local, nct, acc, red)) {
@@ -114,8 +195,8 @@ __global__ void __launch_bounds__(N / 16) k_rowi_p2(const GridDev* __restrict__ 
 
 // MODE 0: DCT initial solve (always runs); MODE 1: PCG (gated).
 template <int N, int NSEQ, int MODE>
-__global__ void __launch_bounds__(N / 16 * NSEQ) k_col_p2(const GridDev* __restrict__ grids,
-                                                          const int* __restrict__ starts, int n) {
+__global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_col_p2(
+    const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
     constexpr int T = N / 16;
     extern __shared__ float2 sm[];
     const int g = find_grid(starts, n, blockIdx.x);
@@ -127,43 +208,45 @@ __global__ void __launch_bounds__(N / 16 * NSEQ) k_col_p2(const GridDev* __restr
     const int s = threadIdx.x % NSEQ, t = threadIdx.x / NSEQ;
     const int ja = 2 * NSEQ * local + 2 * s;
     const bool hasa = ja < W, hasb = ja + 1 < W;
+    const bool vec = hasb && !(P & 1);
     float2* sms = sm + s * RegFft<N>::SMEM;
     float* __restrict__ Tm = G.T;
-    float2 v[16];
-#pragma unroll
+#pragma unroll 4
     for (int q = 0; q < 16; q++) {
-        const size_t o = (size_t)mk_src<N>(t + T * q) * P + ja;
+        const int m = t + T * q;
+        const size_t o = (size_t)mk_src<N>(m) * P + ja;
         float2 x = make_float2(0.f, 0.f);
-        if (hasb && !(P & 1)) x = *reinterpret_cast<const float2*>(Tm + o);
+        if (vec) x = *reinterpret_cast<const float2*>(Tm + o);
         else if (hasb) x = make_float2(Tm[o], Tm[o + 1]);
         else if (hasa) x.x = Tm[o];
-        v[q] = x;
+        sms[pad16(m)] = x;
     }
-    const float2* __restrict__ tw = G.pcol.fft.tw;
-    reg_fft<N>(v, sms, t, tw);
-#pragma unroll
-    for (int q = 0; q < 16; q++) sms[pad16(t + T * q)] = v[q];
     __syncthreads();
+    const float2* __restrict__ tw = G.pcol.fft.tw;
+    smem_fft<N>(sms, t, tw);
     const float2* __restrict__ dw = G.pcol.dctw;
     const double* __restrict__ cH = G.cosH;
     const double ca = hasa ? G.cosW[ja] : 1.0, cb = hasb ? G.cosW[ja + 1] : 1.0;
     const float negs = -1.0f / (4.0f * (float)N * (float)W);
-#pragma unroll
-    for (int q = 0; q < 16; q++) {
-        const int k = t + T * q;
+    for (int k = t; k <= N / 2; k += T) {
         const int km = (N - k) & (N - 1);
-        const float2 Cm = sms[pad16(km)];
-        v[q] = col_spectral(v[q], Cm, k, km, __ldg(&dw[k]), __ldg(&dw[km]), cH[k], cH[km], ca, cb, ja == 0, hasb,
-                            negs);
+        const float2 C = sms[pad16(k)], Cm = sms[pad16(km)];
+        const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
+        const double ck = cH[k], cm = cH[km];
+        const float2 ok = col_spectral(C, Cm, k, km, wk, wm, ck, cm, ca, cb, ja == 0, hasb, negs);
+        if (km != k) sms[pad16(km)] = col_spectral(Cm, C, km, k, wm, wk, cm, ck, ca, cb, ja == 0, hasb, negs);
+        sms[pad16(k)] = ok;
     }
     __syncthreads();
-    reg_fft<N>(v, sms, t, tw);
-#pragma unroll
+    smem_fft<N>(sms, t, tw);
+#pragma unroll 4
     for (int q = 0; q < 16; q++) {
-        const size_t o = (size_t)mk_src<N>(t + T * q) * P + ja;
-        if (hasb && !(P & 1)) *reinterpret_cast<float2*>(Tm + o) = make_float2(v[q].x, -v[q].y);
-        else if (hasb) { Tm[o] = v[q].x; Tm[o + 1] = -v[q].y; }
-        else if (hasa) Tm[o] = v[q].x;
+        const int m = t + T * q;
+        const size_t o = (size_t)mk_src<N>(m) * P + ja;
+        const float2 v = sms[pad16(m)];
+        if (vec) *reinterpret_cast<float2*>(Tm + o) = make_float2(v.x, -v.y);
+        else if (hasb) { Tm[o] = v.x; Tm[o + 1] = -v.y; }
+        else if (hasa) Tm[o] = v.x;
     }
 }
 
@@ -230,15 +313,15 @@ int unw_p2_col_nseq(int N) {
     }
 }
 
-#define UNW_P2_SWITCH(N, CALL)          \
-    switch (N) {                        \
-        case 256: return CALL(256);     \
-        case 512: return CALL(512);     \
-        case 1024: return CALL(1024);   \
-        case 2048: return CALL(2048);   \
-        case 4096: return CALL(4096);   \
-        case 8192: return CALL(8192);   \
-        case 16384: return CALL(16384); \
+#define UNW_P2_SWITCH(N, CALL)                 \
+    switch (N) {                               \
+        case 256: return CALL(256);            \
+        case 512: return CALL(512);            \
+        case 1024: return CALL(1024);          \
+        case 2048: return CALL(2048);          \
+        case 4096: return CALL(4096);          \
+        case 8192: return CALL(8192);          \
+        case 16384: return CALL(16384);        \
         default: return cudaErrorInvalidValue; \
     }
 

@@ -27,6 +27,30 @@ struct RegFft {
     static constexpr int SMEM = N + N / 16;       // float2 slots per sequence
 };
 
+// Multiplies w[r] by w1^r, r = 1..R-1, from a single table twiddle w1: powers
+// by squaring (w2, w4, w8) and one extra product each, so every power carries
+// at most a few roundings (relative error below 1e-6).
+template <int R>
+__device__ __forceinline__ void twiddle_row(float2* w, float2 w1) {
+    float2 p[R];
+    p[1] = w1;
+    if (R > 2) p[2] = cmul(w1, w1);
+    if (R > 3) p[3] = cmul(p[2], w1);
+    if (R > 4) {
+        p[4] = cmul(p[2], p[2]);
+        p[5] = cmul(p[4], w1);
+        p[6] = cmul(p[4], p[2]);
+        p[7] = cmul(p[4], p[3]);
+    }
+    if (R > 8) {
+        p[8] = cmul(p[4], p[4]);
+#pragma unroll
+        for (int r = 9; r < R; r++) p[r] = cmul(p[8], p[r - 8]);
+    }
+#pragma unroll
+    for (int r = 1; r < R; r++) w[r] = cmul(w[r], p[r]);
+}
+
 // One Stockham pass of radix R with NS = product of earlier radices.
 // Butterfly j = t + b*T (b < 16/R) reads elements j + r*(N/R) and writes
 // (j - k)*R + k + r*NS, k = j mod NS.
@@ -51,10 +75,7 @@ __device__ __forceinline__ void reg_pass(float2 (&v)[16], float2* __restrict__ s
     for (int b = 0; b < NB; b++) {
         const int j = t + b * T;
         const int k = j & (NS - 1);
-        if (NS > 1) {
-#pragma unroll
-            for (int r = 1; r < R; r++) w[b][r] = cmul(w[b][r], __ldg(&tw[r * k * S]));
-        }
+        if (NS > 1) twiddle_row<R>(w[b], __ldg(&tw[k * S]));
         Dft<R>::run(w[b]);
         if (LAST) {
 #pragma unroll
@@ -75,6 +96,25 @@ __device__ __forceinline__ void reg_fft_rec(float2 (&v)[16], float2* sm, int t, 
         reg_pass<N, R, NS, P == 0, P == RegFft<N>::NPASS - 1>(v, sm, t, tw);
         reg_fft_rec<N, P + 1, NS * R>(v, sm, t, tw);
     }
+}
+
+template <int N, int P, int NS>
+__device__ __forceinline__ void smem_fft_rec(float2* sm, int t, const float2* tw) {
+    if constexpr (P < RegFft<N>::NPASS) {
+        constexpr int R = (P < RegFft<N>::NP16) ? 16 : (1 << RegFft<N>::REM);
+        float2 v[16];
+        reg_pass<N, R, NS, false, false>(v, sm, t, tw);
+        smem_fft_rec<N, P + 1, NS * R>(sm, t, tw);
+    }
+}
+
+// Forward FFT of the sequence held in shared memory (natural order, padded
+// addresses pad16(i)), result in place.  Registers are used only inside each
+// pass.  The caller synchronises before the call (inputs written) and the
+// result is visible to all threads on return.
+template <int N>
+__device__ __forceinline__ void smem_fft(float2* sm, int t, const float2* tw) {
+    smem_fft_rec<N, 0, 1>(sm, t, tw);
 }
 
 // Forward FFT (exp(-2 pi i nk/N)) in place in the stride-T register layout.

@@ -329,9 +329,11 @@ __device__ __forceinline__ float pnew1(const float* __restrict__ z, const float*
     return first ? z[o] : fadd(fmul(po[o], beta), z[o]);
 }
 
-// matvec: p = z + beta p_old, Ap = A p, pAp = p.Ap (utils_unwrap2d.py:1430-1443, :1471)
-__global__ void __launch_bounds__(256) k_matvec(const GridDev* __restrict__ grids,
-                                                const int* __restrict__ starts, int n, int k) {
+// matvec: p = z + beta p_old, Ap = A p, pAp = p.Ap (utils_unwrap2d.py:1430-1443, :1471).
+// Software-pipelined one row ahead: the loads of row i+2 (z, p_old) and of the
+// weights of row i+1 are issued before row i is computed.
+__global__ void __launch_bounds__(256, 3) k_matvec(const GridDev* __restrict__ grids,
+                                                   const int* __restrict__ starts, int n, int k) {
     __shared__ double red[32 * 1];
     const int g = find_grid(starts, n, blockIdx.x);
     const GridDev& G = grids[g];
@@ -355,19 +357,30 @@ __global__ void __launch_bounds__(256) k_matvec(const GridDev* __restrict__ grid
     // lanes past the last column load nothing (j0 < W implies j0 + 3 < P)
     const bool lane_on = j0 < W;
     if (ib < H) {
-        F4 up{}, wyu{}, cur{}, dn{};
+        F4 up{}, wyu{}, cur{}, dn{}, wx{}, wy{};
+        F4 nz{}, npo{}, nwx{}, nwy{};
         size_t o = (size_t)ib * P + j0;
-        if (lane_on) cur = pnew4(z, po, o, first, beta);
-        if (ib > 0 && lane_on) {
-            up = pnew4(z, po, o - P, first, beta);
-            wyu = ld4(wIy, o - P);
+        if (lane_on) {
+            cur = pnew4(z, po, o, first, beta);
+            if (ib > 0) {
+                up = pnew4(z, po, o - P, first, beta);
+                wyu = ld4(wIy, o - P);
+            }
+            if (ib < H - 1) dn = pnew4(z, po, o + P, first, beta);
+            wx = ld4(wIx, o);
+            wy = ld4(wIy, o);
         }
         for (int i = ib; i < ie; i++, o += P) {
-            F4 wx{}, wy{};
+            // prefetch: p inputs of row i+2, weights of row i+1
             if (lane_on) {
-                if (i < H - 1) dn = pnew4(z, po, o + P, first, beta);
-                wx = ld4(wIx, o);
-                wy = ld4(wIy, o);
+                if (i + 2 < H) {
+                    nz = ld4(z, o + 2 * (size_t)P);
+                    if (!first) npo = ld4(po, o + 2 * (size_t)P);
+                }
+                if (i + 1 < H) {
+                    nwx = ld4(wIx, o + P);
+                    nwy = ld4(wIy, o + P);
+                }
             }
             float pl = __shfl_up_sync(0xffffffffu, cur.v[3], 1);
             float wl = __shfl_up_sync(0xffffffffu, wx.v[3], 1);
@@ -400,6 +413,14 @@ __global__ void __launch_bounds__(256) k_matvec(const GridDev* __restrict__ grid
             up = cur;
             cur = dn;
             wyu = wy;
+            wx = nwx;
+            wy = nwy;
+            if (!first) {
+#pragma unroll
+                for (int c = 0; c < 4; c++) dn.v[c] = fadd(fmul(npo.v[c], beta), nz.v[c]);
+            } else {
+                dn = nz;
+            }
         }
     }
     if (arrive<1>(G, local, nct, acc, red)) {
