@@ -138,10 +138,11 @@ __device__ __forceinline__ float2 col_spectral(float2 C, float2 Cm, int k, int k
     float Xam = wm.x * Vam.x - wm.y * Vam.y, Xbm = wm.x * Vbm.x - wm.y * Vbm.y;
     const float lak = (float)(2.0 * ck + 2.0 * ca - 4.0), lbk = (float)(2.0 * ck + 2.0 * cb - 4.0);
     const float lam = (float)(2.0 * cm + 2.0 * ca - 4.0), lbm = (float)(2.0 * cm + 2.0 * cb - 4.0);
-    Xak = (k == 0 && ja0) ? 0.f : fdiv(Xak, lak) * negs;
-    Xam = (km == 0 && ja0) ? 0.f : fdiv(Xam, lam) * negs;
-    Xbk = hasb ? fdiv(Xbk, lbk) * negs : 0.f;
-    Xbm = hasb ? fdiv(Xbm, lbm) * negs : 0.f;
+    // X / lambda as X * (1/lambda) with a correctly rounded reciprocal
+    Xak = (k == 0 && ja0) ? 0.f : Xak * __frcp_rn(lak) * negs;
+    Xam = (km == 0 && ja0) ? 0.f : Xam * __frcp_rn(lam) * negs;
+    Xbk = hasb ? Xbk * __frcp_rn(lbk) * negs : 0.f;
+    Xbm = hasb ? Xbm * __frcp_rn(lbm) * negs : 0.f;
     const float mak = k == 0 ? 0.f : Xam, mbk = k == 0 ? 0.f : Xbm;
     const float2 Pak = cmul(cconj(wk), make_float2(Xak, -mak));
     const float2 Pbk = cmul(cconj(wk), make_float2(Xbk, -mbk));

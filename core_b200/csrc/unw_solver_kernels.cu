@@ -359,6 +359,9 @@ __global__ void __launch_bounds__(256, 3) k_matvec(const GridDev* __restrict__ g
     if (ib < H) {
         F4 up{}, wyu{}, cur{}, dn{}, wx{}, wy{};
         F4 nz{}, npo{}, nwx{}, nwy{};
+        // tile-edge scalars (column j0-1 for lane 0, j0+4 for lane 31) of the current row
+        const bool eleft = lane == 0 && j0 > 0, eright = lane == 31 && j0 + 4 < W;
+        float epl = 0.f, ewl = 0.f, epr = 0.f, npl = 0.f, nwl = 0.f, npr = 0.f;
         size_t o = (size_t)ib * P + j0;
         if (lane_on) {
             cur = pnew4(z, po, o, first, beta);
@@ -370,8 +373,10 @@ __global__ void __launch_bounds__(256, 3) k_matvec(const GridDev* __restrict__ g
             wx = ld4(wIx, o);
             wy = ld4(wIy, o);
         }
+        if (eleft) { epl = pnew1(z, po, o - 1, first, beta); ewl = wIx[o - 1]; }
+        if (eright) epr = pnew1(z, po, o + 4, first, beta);
         for (int i = ib; i < ie; i++, o += P) {
-            // prefetch: p inputs of row i+2, weights of row i+1
+            // prefetch: p inputs of row i+2, weights and edge scalars of row i+1
             if (lane_on) {
                 if (i + 2 < H) {
                     nz = ld4(z, o + 2 * (size_t)P);
@@ -382,14 +387,15 @@ __global__ void __launch_bounds__(256, 3) k_matvec(const GridDev* __restrict__ g
                     nwy = ld4(wIy, o + P);
                 }
             }
+            if (i + 1 < H) {
+                if (eleft) { npl = pnew1(z, po, o + P - 1, first, beta); nwl = wIx[o + P - 1]; }
+                if (eright) npr = pnew1(z, po, o + P + 4, first, beta);
+            }
             float pl = __shfl_up_sync(0xffffffffu, cur.v[3], 1);
             float wl = __shfl_up_sync(0xffffffffu, wx.v[3], 1);
             float pr = __shfl_down_sync(0xffffffffu, cur.v[0], 1);
-            if (lane == 0 && j0 > 0) {
-                pl = pnew1(z, po, o - 1, first, beta);
-                wl = wIx[o - 1];
-            }
-            if (lane == 31 && j0 + 4 < W) pr = pnew1(z, po, o + 4, first, beta);
+            if (eleft) { pl = epl; wl = ewl; }
+            if (eright) pr = epr;
             F4 ap;
 #pragma unroll
             for (int c = 0; c < 4; c++) {
@@ -415,6 +421,9 @@ __global__ void __launch_bounds__(256, 3) k_matvec(const GridDev* __restrict__ g
             wyu = wy;
             wx = nwx;
             wy = nwy;
+            epl = npl;
+            ewl = nwl;
+            epr = npr;
             if (!first) {
 #pragma unroll
                 for (int c = 0; c < 4; c++) dn.v[c] = fadd(fmul(npo.v[c], beta), nz.v[c]);
