@@ -133,7 +133,7 @@ GridLayout grid_layout(long long H0, long long W0) {
     auto take = [&](size_t bytes) { size_t r = o; o = up(o + bytes, ALIGN); return r; };
     L.P0 = (long long)up((size_t)W0, 32);
     const size_t A = (size_t)H0 * (size_t)L.P0 * sizeof(float);
-    L.max_ctas = std::max<long long>({(H0 + 1) / 2, (W0 + 1) / 2, ((W0 + 127) / 128) * ((H0 + 15) / 16),
+    L.max_ctas = std::max<long long>({(H0 + 1) / 2, (W0 + 1) / 2, ((W0 + 127) / 128) * ((H0 + 7) / 8),
                                       ELEM_MAX_CTAS});
     L.fr_cap = (int)std::max<long long>(next_smooth(2 * W0 - 1), W0);
     L.fc_cap = (int)std::max<long long>(next_smooth(2 * H0 - 1), H0);
@@ -268,6 +268,7 @@ int kind_ctas(const GridDev& G, int kind) {
         case KS_ROWPAIR: return (G.H + 1) / 2;
         case KS_COL: return (G.W + 2 * G.col_nseq - 1) / (2 * G.col_nseq);
         case KS_STEN: return G.sten_tiles_x * ((G.H + 8 * G.sten_rows - 1) / (8 * G.sten_rows));
+        case KS_MATVEC: return G.sten_tiles_x * ((G.H + 15) / 16);
         case KS_ELEM: return elem_ctas(npx);
         case KS_ONE: return 1;
         default: return (int)((npx + 4095) / 4096);  // post tiles
@@ -302,7 +303,7 @@ int enqueue_iteration(Solver& S, int t) {
     PL(UNW_PROF_COL, L_col(S, 1));
     PL(UNW_PROF_ROW_INV, L_rowi(S, 1));
     for (int k = 0; k < S.sc.cg_max_iter; k++) {
-        PL(UNW_PROF_MATVEC, unw_launch_simple(UNW_K_MATVEC, S.total[KS_STEN], s, S.dg, S.ds(KS_STEN), n, k, S.sc));
+        PL(UNW_PROF_MATVEC, unw_launch_simple(UNW_K_MATVEC, S.total[KS_MATVEC], s, S.dg, S.ds(KS_MATVEC), n, k, S.sc));
         PL(UNW_PROF_ROW_UPD, L_rowf(S, 2, t, k));
         PL(UNW_PROF_COL, L_col(S, 1));
         PL(UNW_PROF_ROW_INV, L_rowi(S, 2));
@@ -423,7 +424,7 @@ int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbo
         S.sh.row_smem = std::max(S.sh.row_smem, (size_t)prow[g].n * sizeof(float2));
         S.sh.col_smem = std::max(S.sh.col_smem, (size_t)nseq * pcol[g].n * sizeof(float2));
         G.sten_tiles_x = (G.W + 127) / 128;
-        G.sten_rows = (int)std::max<long long>(2, std::min<long long>(16, (long long)G.sten_tiles_x * G.H / 4800));
+        G.sten_rows = 1;
     }
     // power-of-two register-FFT paths when every grid shares the dimension
     {

@@ -209,9 +209,9 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
     const int ja = 2 * NSEQ * local + 2 * s;
     const bool hasa = ja < W, hasb = ja + 1 < W;
     const bool vec = hasb && !(P & 1);
-    float2* sms = sm + s * RegFft<N>::SMEM;
+    float2* sms = sm + s * RegFft<N>::SEQ_STRIDE;
     float* __restrict__ Tm = G.T;
-#pragma unroll 4
+#pragma unroll
     for (int q = 0; q < 16; q++) {
         const int m = t + T * q;
         const size_t o = (size_t)mk_src<N>(m) * P + ja;
@@ -232,14 +232,14 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
         const int km = (N - k) & (N - 1);
         const float2 C = sms[pad16(k)], Cm = sms[pad16(km)];
         const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
-        const double ck = cH[k], cm = cH[km];
+        const double ck = __ldg(&cH[k]), cm = __ldg(&cH[km]);
         const float2 ok = col_spectral(C, Cm, k, km, wk, wm, ck, cm, ca, cb, ja == 0, hasb, negs);
         if (km != k) sms[pad16(km)] = col_spectral(Cm, C, km, k, wm, wk, cm, ck, ca, cb, ja == 0, hasb, negs);
         sms[pad16(k)] = ok;
     }
     __syncthreads();
     smem_fft<N>(sms, t, tw);
-#pragma unroll 4
+#pragma unroll
     for (int q = 0; q < 16; q++) {
         const int m = t + T * q;
         const size_t o = (size_t)mk_src<N>(m) * P + ja;
@@ -291,7 +291,7 @@ constexpr int col_nseq_p2() { return N >= 8192 ? 1 : (8192 / N > 8 ? 8 : 8192 / 
 template <int N>
 static cudaError_t col_p2_n(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* st, int n) {
     constexpr int NS = col_nseq_p2<N>();
-    const size_t smem = sizeof(float2) * RegFft<N>::SMEM * NS;
+    const size_t smem = sizeof(float2) * RegFft<N>::SEQ_STRIDE * NS;
     auto go = [&](auto kfn) {
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kfn<<<nblk, N / 16 * NS, smem, s>>>(gd, st, n);

@@ -14,7 +14,7 @@
 #define UNW_MAX_LOG 64       // per-IRLS-iteration CG counts kept in the state
 
 // Kernel shapes; each has its own CTA prefix array.
-enum { KS_ROWPAIR = 0, KS_COL = 1, KS_STEN = 2, KS_ELEM = 3, KS_ONE = 4, KS_NKIND = 5 };
+enum { KS_ROWPAIR = 0, KS_COL = 1, KS_STEN = 2, KS_ELEM = 3, KS_ONE = 4, KS_MATVEC = 5, KS_NKIND = 6 };
 
 struct FftPlanDev {
     int n;                      // transform length

@@ -25,6 +25,9 @@ struct RegFft {
     static constexpr int REM = LOG % 4;           // log2 of the final small radix (0 = none)
     static constexpr int NPASS = NP16 + (REM ? 1 : 0);
     static constexpr int SMEM = N + N / 16;       // float2 slots per sequence
+    // distance between sequences sharing a CTA: SMEM + 8 float2, so that lanes of
+    // two sequences at the same position fall on different banks (16 words apart)
+    static constexpr int SEQ_STRIDE = SMEM + 8;
 };
 
 // Multiplies w[r] by w1^r, r = 1..R-1, from a single table twiddle w1: powers
@@ -61,13 +64,16 @@ __device__ __forceinline__ void reg_pass(float2 (&v)[16], float2* __restrict__ s
     constexpr int NB = 16 / R;
     constexpr int NR = N / R;
     constexpr int S = N / (NS * R);
+    // padded addresses with compile-time strides: pad16(a + 16 c) = pad16(a) + 17 c
+    static_assert(T % 16 == 0 && NR % 16 == 0, "strides must be multiples of 16");
     float2 w[NB][R];
+    const int rd = pad16(t);
 #pragma unroll
     for (int b = 0; b < NB; b++) {
 #pragma unroll
         for (int r = 0; r < R; r++) {
             if (FIRST) w[b][r] = v[b + r * NB];
-            else w[b][r] = sm[pad16(t + b * T + r * NR)];
+            else w[b][r] = sm[rd + b * (T + T / 16) + r * (NR + NR / 16)];
         }
     }
     if (!FIRST) __syncthreads();  // every read of this exchange done before it is overwritten
@@ -82,8 +88,16 @@ __device__ __forceinline__ void reg_pass(float2 (&v)[16], float2* __restrict__ s
             for (int r = 0; r < R; r++) v[b + r * NB] = w[b][r];
         } else {
             const int base = (j - k) * R + k;
+            if (NS == 1) {
+                static_assert(NS > 1 || R == 16, "first pass is radix 16");
+                // pad16(16 j + r) = 17 j + r for r < 16
 #pragma unroll
-            for (int r = 0; r < R; r++) sm[pad16(base + r * NS)] = w[b][r];
+                for (int r = 0; r < R; r++) sm[17 * j + r] = w[b][r];
+            } else {
+                const int wb = pad16(base);
+#pragma unroll
+                for (int r = 0; r < R; r++) sm[wb + r * (NS + NS / 16)] = w[b][r];
+            }
         }
     }
     if (!LAST) __syncthreads();

@@ -330,9 +330,11 @@ __device__ __forceinline__ float pnew1(const float* __restrict__ z, const float*
 }
 
 // matvec: p = z + beta p_old, Ap = A p, pAp = p.Ap (utils_unwrap2d.py:1430-1443, :1471).
-// Software-pipelined one row ahead: the loads of row i+2 (z, p_old) and of the
-// weights of row i+1 are issued before row i is computed.
-__global__ void __launch_bounds__(256, 3) k_matvec(const GridDev* __restrict__ grids,
+// A CTA is 16 warps over a 128-column x 16-row tile; each warp computes one row
+// (4 columns per lane) and issues all its loads (rows i-1, i, i+1 of z and
+// p_old, the weights, the tile-edge scalars) before using any of them.  The
+// neighbouring rows come back from L1/L2: DRAM traffic stays one pass per array.
+__global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ grids,
                                                    const int* __restrict__ starts, int n, int k) {
     __shared__ double red[32 * 1];
     const int g = find_grid(starts, n, blockIdx.x);
@@ -345,92 +347,76 @@ __global__ void __launch_bounds__(256, 3) k_matvec(const GridDev* __restrict__ g
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tx = local % G.sten_tiles_x, ty = local / G.sten_tiles_x;
     const int j0 = tx * 128 + lane * 4;
-    const int ib = (ty * 8 + warp) * G.sten_rows, ie = min(H, ib + G.sten_rows);
+    const int i = ty * 16 + warp;
     const bool first = st->pfirst != 0;
     const float beta = st->beta;
     const float* __restrict__ z = G.z;
     const float* __restrict__ po = (k & 1) ? G.p0 : G.p1;
     float* __restrict__ pn = (k & 1) ? G.p1 : G.p0;
-    const float* __restrict__ wIx = G.wIx;
-    const float* __restrict__ wIy = G.wIy;
     double acc[1] = {0.0};
     // lanes past the last column load nothing (j0 < W implies j0 + 3 < P)
-    const bool lane_on = j0 < W;
-    if (ib < H) {
-        F4 up{}, wyu{}, cur{}, dn{}, wx{}, wy{};
-        F4 nz{}, npo{}, nwx{}, nwy{};
-        // tile-edge scalars (column j0-1 for lane 0, j0+4 for lane 31) of the current row
-        const bool eleft = lane == 0 && j0 > 0, eright = lane == 31 && j0 + 4 < W;
-        float epl = 0.f, ewl = 0.f, epr = 0.f, npl = 0.f, nwl = 0.f, npr = 0.f;
-        size_t o = (size_t)ib * P + j0;
-        if (lane_on) {
-            cur = pnew4(z, po, o, first, beta);
-            if (ib > 0) {
-                up = pnew4(z, po, o - P, first, beta);
-                wyu = ld4(wIy, o - P);
-            }
-            if (ib < H - 1) dn = pnew4(z, po, o + P, first, beta);
-            wx = ld4(wIx, o);
-            wy = ld4(wIy, o);
+    const bool on = i < H && j0 < W;
+    const bool hu = i > 0, hd = i < H - 1;
+    const size_t o = (size_t)i * P + j0;
+    F4 zc{}, zu{}, zd{}, qc{}, qu{}, qd{}, wx{}, wy{}, wyu{};
+    float zl = 0.f, ql = 0.f, wl = 0.f, zr = 0.f, qr = 0.f;
+    if (on) {
+        zc = ld4(z, o);
+        if (hu) zu = ld4(z, o - P);
+        if (hd) zd = ld4(z, o + P);
+        if (!first) {
+            qc = ld4(po, o);
+            if (hu) qu = ld4(po, o - P);
+            if (hd) qd = ld4(po, o + P);
         }
-        if (eleft) { epl = pnew1(z, po, o - 1, first, beta); ewl = wIx[o - 1]; }
-        if (eright) epr = pnew1(z, po, o + 4, first, beta);
-        for (int i = ib; i < ie; i++, o += P) {
-            // prefetch: p inputs of row i+2, weights and edge scalars of row i+1
-            if (lane_on) {
-                if (i + 2 < H) {
-                    nz = ld4(z, o + 2 * (size_t)P);
-                    if (!first) npo = ld4(po, o + 2 * (size_t)P);
-                }
-                if (i + 1 < H) {
-                    nwx = ld4(wIx, o + P);
-                    nwy = ld4(wIy, o + P);
-                }
-            }
-            if (i + 1 < H) {
-                if (eleft) { npl = pnew1(z, po, o + P - 1, first, beta); nwl = wIx[o + P - 1]; }
-                if (eright) npr = pnew1(z, po, o + P + 4, first, beta);
-            }
-            float pl = __shfl_up_sync(0xffffffffu, cur.v[3], 1);
-            float wl = __shfl_up_sync(0xffffffffu, wx.v[3], 1);
-            float pr = __shfl_down_sync(0xffffffffu, cur.v[0], 1);
-            if (eleft) { pl = epl; wl = ewl; }
-            if (eright) pr = epr;
-            F4 ap;
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const int j = j0 + c;
-                const float pc = cur.v[c];
-                const float pleft = c == 0 ? pl : cur.v[c - 1];
-                const float pright = c == 3 ? pr : cur.v[c + 1];
-                const float wleft = c == 0 ? wl : wx.v[c - 1];
-                float res = 0.f;
-                if (j > 0) res = fsub(res, fmul(fsub(pc, pleft), wleft));
-                if (j < W - 1) res = fadd(res, fmul(fsub(pright, pc), wx.v[c]));
-                if (i > 0) res = fsub(res, fmul(fsub(pc, up.v[c]), wyu.v[c]));
-                if (i < H - 1) res = fadd(res, fmul(fsub(dn.v[c], pc), wy.v[c]));
-                ap.v[c] = -res;
-                if (j < W) acc[0] += (double)pc * (double)ap.v[c];
-            }
-            if (lane_on) {
-                st4(pn, o, cur);
-                st4(G.Ap, o, ap);
-            }
-            up = cur;
-            cur = dn;
-            wyu = wy;
-            wx = nwx;
-            wy = nwy;
-            epl = npl;
-            ewl = nwl;
-            epr = npr;
-            if (!first) {
-#pragma unroll
-                for (int c = 0; c < 4; c++) dn.v[c] = fadd(fmul(npo.v[c], beta), nz.v[c]);
-            } else {
-                dn = nz;
-            }
+        wx = ld4(G.wIx, o);
+        wy = ld4(G.wIy, o);
+        if (hu) wyu = ld4(G.wIy, o - P);
+        if (lane == 0 && j0 > 0) {
+            zl = z[o - 1];
+            if (!first) ql = po[o - 1];
+            wl = G.wIx[o - 1];
         }
+        if (lane == 31 && j0 + 4 < W) {
+            zr = z[o + 4];
+            if (!first) qr = po[o + 4];
+        }
+    }
+    F4 cur = zc, up = zu, dn = zd;
+    if (!first) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            cur.v[c] = fadd(fmul(qc.v[c], beta), zc.v[c]);
+            up.v[c] = fadd(fmul(qu.v[c], beta), zu.v[c]);
+            dn.v[c] = fadd(fmul(qd.v[c], beta), zd.v[c]);
+        }
+        zl = fadd(fmul(ql, beta), zl);
+        zr = fadd(fmul(qr, beta), zr);
+    }
+    float pl = __shfl_up_sync(0xffffffffu, cur.v[3], 1);
+    float wll = __shfl_up_sync(0xffffffffu, wx.v[3], 1);
+    float pr = __shfl_down_sync(0xffffffffu, cur.v[0], 1);
+    if (lane == 0) { pl = zl; wll = wl; }
+    if (lane == 31) pr = zr;
+    if (on) {
+        F4 ap;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int j = j0 + c;
+            const float pc = cur.v[c];
+            const float pleft = c == 0 ? pl : cur.v[c - 1];
+            const float pright = c == 3 ? pr : cur.v[c + 1];
+            const float wleft = c == 0 ? wll : wx.v[c - 1];
+            float res = 0.f;
+            if (j > 0) res = fsub(res, fmul(fsub(pc, pleft), wleft));
+            if (j < W - 1) res = fadd(res, fmul(fsub(pright, pc), wx.v[c]));
+            if (hu) res = fsub(res, fmul(fsub(pc, up.v[c]), wyu.v[c]));
+            if (hd) res = fadd(res, fmul(fsub(dn.v[c], pc), wy.v[c]));
+            ap.v[c] = -res;
+            if (j < W) acc[0] += (double)pc * (double)ap.v[c];
+        }
+        st4(pn, o, cur);
+        st4(G.Ap, o, ap);
     }
     if (arrive<1>(G, local, nct, acc, red)) {
         finish_sum<1>(G, nct, acc, red);
@@ -752,7 +738,7 @@ cudaError_t unw_launch_simple(int which, int nblk, cudaStream_t s, const GridDev
     switch (which) {
         case UNW_K_STATE_INIT: k_state_init<<<(n + 63) / 64, 64, 0, s>>>(gd, n, sc); break;
         case UNW_K_SETUP: k_setup<<<nblk, 256, 0, s>>>(gd, starts, n); break;
-        case UNW_K_MATVEC: k_matvec<<<nblk, 256, 0, s>>>(gd, starts, n, it); break;
+        case UNW_K_MATVEC: k_matvec<<<nblk, 512, 0, s>>>(gd, starts, n, it); break;
         case UNW_K_HEAD: k_head<<<nblk, 256, 0, s>>>(gd, starts, n, it); break;
         case UNW_K_MEAN: k_mean<<<nblk, 256, 0, s>>>(gd, starts, n, it); break;
         case UNW_K_INIT_RECENTRE: k_init_recentre<<<nblk, 256, 0, s>>>(gd, starts, n); break;
