@@ -54,6 +54,10 @@ constexpr int HIST_CAP = 65536;
 constexpr int ELEM_MAX_CTAS = 1184;      // 8 x 148 SMs
 constexpr size_t COL_SMEM_BUDGET = 96 * 1024;
 constexpr int MAX_FFT = 16384;           // longest transform one CTA holds (1024 threads x 16)
+// CTAs of the persistent PCG kernels (148 SMs x resident CTAs per SM)
+constexpr int CTAS_ROW = 148 * 4;
+constexpr int CTAS_COL = 148 * 2;
+constexpr int CTAS_MATVEC = 148 * 2;
 
 size_t up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -144,12 +148,12 @@ GridLayout grid_layout(long long H0, long long W0) {
     L.hs_r = take(sizeof(float2) * L.fr_cap);
     L.dw_r = take(sizeof(float2) * W0);
     L.ch_r = take(sizeof(float2) * W0);
-    L.cos_r = take(sizeof(double) * W0);
+    L.cos_r = take(sizeof(float) * W0);
     L.tw_c = take(sizeof(float2) * L.fc_cap);
     L.hs_c = take(sizeof(float2) * L.fc_cap);
     L.dw_c = take(sizeof(float2) * H0);
     L.ch_c = take(sizeof(float2) * H0);
-    L.cos_c = take(sizeof(double) * H0);
+    L.cos_c = take(sizeof(float) * H0);
     for (int a = 0; a < 16; a++) L.arr[a] = take(A);
     L.valid = take((size_t)H0 * L.P0);
     L.hist = take(sizeof(int) * HIST_CAP);
@@ -265,10 +269,11 @@ int kind_ctas(const GridDev& G, int kind) {
     if (G.H == 0) return 0;
     const long long npx = (long long)G.H * G.W;
     switch (kind) {
-        case KS_ROWPAIR: return (G.H + 1) / 2;
-        case KS_COL: return (G.W + 2 * G.col_nseq - 1) / (2 * G.col_nseq);
+        // persistent kinds: at most a few CTAs per SM, each loops over its units
+        case KS_ROWPAIR: return std::min((G.H + 1) / 2, CTAS_ROW);
+        case KS_COL: return std::min((G.W + 2 * G.col_nseq - 1) / (2 * G.col_nseq), CTAS_COL);
         case KS_STEN: return G.sten_tiles_x * ((G.H + 8 * G.sten_rows - 1) / (8 * G.sten_rows));
-        case KS_MATVEC: return G.sten_tiles_x * ((G.H + 15) / 16);
+        case KS_MATVEC: return std::min(G.sten_tiles_x * ((G.H + 15) / 16), CTAS_MATVEC);
         case KS_ELEM: return elem_ctas(npx);
         case KS_ONE: return 1;
         default: return (int)((npx + 4095) / 4096);  // post tiles
@@ -372,8 +377,8 @@ int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbo
                             &G.z, &G.p0, &G.p1, &G.Ap, &G.T, &G.U0, &G.U1, &G.Ub};
         for (int a = 0; a < 16; a++) *arrs[a] = (float*)(gb + L.arr[a]);
         G.valid = (uint8_t*)(gb + L.valid);
-        G.cosH = (const double*)(gb + L.cos_c);
-        G.cosW = (const double*)(gb + L.cos_r);
+        G.sH = (const float*)(gb + L.cos_c);
+        G.sW = (const float*)(gb + L.cos_r);
         G.hist = (int*)(gb + L.hist);
         G.hist_cap = HIST_CAP;
         G.tilecnt = (int*)(gb + L.tilecnt);
@@ -463,8 +468,8 @@ int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbo
     for (int g = 0; g < n; g++) {
         GridDev& G = S.hg[g];
         if (G.H == 0) continue;
-        CK(unw_launch_tables(G.prow.fft, G.prow, const_cast<double*>(G.cosW), G.W, s));
-        CK(unw_launch_tables(G.pcol.fft, G.pcol, const_cast<double*>(G.cosH), G.H, s));
+        CK(unw_launch_tables(G.prow.fft, G.prow, const_cast<float*>(G.sW), G.W, s));
+        CK(unw_launch_tables(G.pcol.fft, G.pcol, const_cast<float*>(G.sH), G.H, s));
         if (G.prow.blue) CK(unw_launch_hspec(pick_threads(prow[g].n, prow[g].cap), EMAX, G.prow, s));
         if (G.pcol.blue) CK(unw_launch_hspec(pick_threads(pcol[g].n, pcol[g].cap), EMAX, G.pcol, s));
         CK(cudaMemsetAsync(G.hist, 0, sizeof(int) * HIST_CAP, s));

@@ -72,13 +72,15 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowf_p2(const 
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, P = G.P;
-    const int i0 = 2 * local, i1 = i0 + 1;
-    const bool has1 = i1 < H;
     const int t = threadIdx.x;
     float* U = (it & 1) ? G.U0 : G.U1;
     const float* pk = (MODE == 2) ? ((cgk & 1) ? G.p1 : G.p0) : nullptr;
     const float alpha = (MODE == 2) ? st->alpha : 0.f;
     double acc[2] = {0.0, 0.0};
+    for (int pair = local; pair < (H + 1) / 2; pair += nct) {
+    const int i0 = 2 * pair, i1 = i0 + 1;
+    const bool has1 = i1 < H;
+    __syncthreads();  // previous row pair's reads of sm are done
     for (int c4 = t; c4 < N / 4; c4 += T) {
         const int j = 4 * c4;
         const float4 a = rowf_vals4<MODE>(G, U, pk, alpha, i0, j, acc);
@@ -107,6 +109,7 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowf_p2(const 
         }
         st4f(Ta, 4 * c4, make_float4(xa[0], xa[1], xa[2], xa[3]));
         if (has1) st4f(Tb, 4 * c4, make_float4(xb[0], xb[1], xb[2], xb[3]));
+    }
     }
     if (MODE == 0 || MODE == 3) return;
     if (arrive<2>(G, local, nct, acc, red)) {
@@ -150,12 +153,15 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, P = G.P;
-    const int i0 = 2 * local, i1 = i0 + 1;
-    const bool has1 = i1 < H;
     const int t = threadIdx.x;
+    const float2* __restrict__ dw = G.prow.dctw;
+    double acc[2] = {0.0, 0.0};
+    for (int pair = local; pair < (H + 1) / 2; pair += nct) {
+    const int i0 = 2 * pair, i1 = i0 + 1;
+    const bool has1 = i1 < H;
     const float* __restrict__ Ta = G.T + (size_t)i0 * P;
     const float* __restrict__ Tb = G.T + (size_t)i1 * P;
-    const float2* __restrict__ dw = G.prow.dctw;
+    __syncthreads();  // previous row pair's reads of sm are done
     // DCT-III pre-twiddle: V'_k = conj(w_k) (Y_k - i Y_{N-k}), Y_N = 0; store conj(C')
     for (int c4 = t; c4 < N / 4; c4 += T) {
         const float4 ya = ld4f(Ta, 4 * c4);
@@ -173,7 +179,6 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
     }
     __syncthreads();
     smem_fft<N>(sm, t, G.prow.fft.tw);
-    double acc[2] = {0.0, 0.0};
     for (int c4 = t; c4 < N / 4; c4 += T) {
         const int j = 4 * c4;
         float za[4], zb[4];
@@ -185,6 +190,7 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
         }
         rowi_store4<MODE>(G, i0, j, make_float4(za[0], za[1], za[2], za[3]), acc);
         if (has1) rowi_store4<MODE>(G, i1, j, make_float4(zb[0], zb[1], zb[2], zb[3]), acc);
+    }
     }
     if (MODE == 3) return;
     if (arrive<2>(G, local, nct, acc, red)) {
@@ -204,13 +210,21 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
     const InstState* st = G.st;
     if (MODE == 1 && !(st->irls_active && st->cg_active)) return;
     const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
     const int W = G.W, P = G.P;
     const int s = threadIdx.x % NSEQ, t = threadIdx.x / NSEQ;
-    const int ja = 2 * NSEQ * local + 2 * s;
-    const bool hasa = ja < W, hasb = ja + 1 < W;
-    const bool vec = hasb && !(P & 1);
     float2* sms = sm + s * RegFft<N>::SEQ_STRIDE;
     float* __restrict__ Tm = G.T;
+    const float2* __restrict__ tw = G.pcol.fft.tw;
+    const float2* __restrict__ dw = G.pcol.dctw;
+    const float* __restrict__ sH = G.sH;
+    const float negs = -1.0f / (4.0f * (float)N * (float)W);
+    const int nslab = (W + 2 * NSEQ - 1) / (2 * NSEQ);
+    for (int slab = local; slab < nslab; slab += nct) {
+    const int ja = 2 * NSEQ * slab + 2 * s;
+    const bool hasa = ja < W, hasb = ja + 1 < W;
+    const bool vec = hasb && !(P & 1);
+    __syncthreads();  // previous slab's reads of sm are done
 #pragma unroll
     for (int q = 0; q < 16; q++) {
         const int m = t + T * q;
@@ -222,17 +236,13 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
         sms[pad16(m)] = x;
     }
     __syncthreads();
-    const float2* __restrict__ tw = G.pcol.fft.tw;
     smem_fft<N>(sms, t, tw);
-    const float2* __restrict__ dw = G.pcol.dctw;
-    const double* __restrict__ cH = G.cosH;
-    const double ca = hasa ? G.cosW[ja] : 1.0, cb = hasb ? G.cosW[ja + 1] : 1.0;
-    const float negs = -1.0f / (4.0f * (float)N * (float)W);
+    const float ca = hasa ? G.sW[ja] : 1.0f, cb = hasb ? G.sW[ja + 1] : 1.0f;
     for (int k = t; k <= N / 2; k += T) {
         const int km = (N - k) & (N - 1);
         const float2 C = sms[pad16(k)], Cm = sms[pad16(km)];
         const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
-        const double ck = __ldg(&cH[k]), cm = __ldg(&cH[km]);
+        const float ck = __ldg(&sH[k]), cm = __ldg(&sH[km]);
         const float2 ok = col_spectral(C, Cm, k, km, wk, wm, ck, cm, ca, cb, ja == 0, hasb, negs);
         if (km != k) sms[pad16(km)] = col_spectral(Cm, C, km, k, wm, wk, cm, ck, ca, cb, ja == 0, hasb, negs);
         sms[pad16(k)] = ok;
@@ -247,6 +257,7 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
         if (vec) *reinterpret_cast<float2*>(Tm + o) = make_float2(v.x, -v.y);
         else if (hasb) { Tm[o] = v.x; Tm[o + 1] = -v.y; }
         else if (hasa) Tm[o] = v.x;
+    }
     }
 }
 

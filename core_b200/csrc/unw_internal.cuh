@@ -74,6 +74,7 @@ struct InstState {
     int pad_;
 };
 
+
 struct GridDev {
     int H, W, P;                // cropped grid, pitch of work arrays
     int H0, W0;                 // caller's full grid
@@ -90,8 +91,12 @@ struct GridDev {
     float *wIx, *wIy, *b, *r, *z, *p0, *p1, *Ap, *T;
     float *U0, *U1, *Ub;
     uint8_t* valid;
-    const double* cosH;         // cos(pi*i/H), H entries
-    const double* cosW;         // cos(pi*j/W), W entries
+    // Neumann-Laplacian eigenvalue parts: lambda(k, j) = -(sH[k] + sW[j]) with
+    // sH[k] = 4 sin^2(pi k / 2H), sW[j] = 4 sin^2(pi j / 2W), each computed in
+    // float64 and rounded once.  Equal to 2cos(pi k/H) + 2cos(pi j/W) - 4
+    // (utils_unwrap2d.py:1284-1289) without its cancellation near k = j = 0.
+    const float* sH;
+    const float* sW;
     DctPlanDev prow, pcol;
     InstState* st;
     double* part;               // reduction partials [max CTAs][UNW_NPART]

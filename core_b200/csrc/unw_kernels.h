@@ -25,7 +25,7 @@ enum {
 };
 
 // solver kernels
-cudaError_t unw_launch_tables(const FftPlanDev& f, const DctPlanDev& d, double* cosv, int Ncos,
+cudaError_t unw_launch_tables(const FftPlanDev& f, const DctPlanDev& d, float* sv, int Ncos,
                               cudaStream_t s);
 cudaError_t unw_launch_hspec(int T, int emax, const DctPlanDev& d, cudaStream_t s);
 cudaError_t unw_launch_row_fwd(int mode, int T, int emax, int nblk, size_t smem, cudaStream_t s,

@@ -124,11 +124,12 @@ __device__ __forceinline__ void rowinv_finalize(InstState* st, const double (&ac
 
 // Column-pass spectral step for one frequency pair (k, H-k) of two columns
 // (ja, ja+1) whose DFT outputs are C = C_k and Cm = C_{H-k}: DCT-II extraction,
-// division by the Neumann-Laplacian eigenvalue (computed in float64 and rounded
-// once, as utils_unwrap2d.py:1284-1289 does), negation, DC term zeroed, then
-// the DCT-III pre-twiddle.  Returns conj(C'_k) ready for a forward FFT.
+// division by the Neumann-Laplacian eigenvalue lambda = -(sH + sW) (see
+// GridDev::sH), negation, DC term zeroed, then the DCT-III pre-twiddle.
+// Returns conj(C'_k) ready for a forward FFT.  negs = -1/(4 H W) folds the
+// transform normalisations; with lambda = -(s) the factor is +1/(4 H W s).
 __device__ __forceinline__ float2 col_spectral(float2 C, float2 Cm, int k, int km, float2 wk, float2 wm,
-                                               double ck, double cm, double ca, double cb, bool ja0, bool hasb,
+                                               float ck, float cm, float ca, float cb, bool ja0, bool hasb,
                                                float negs) {
     const float2 Vak = make_float2(C.x + Cm.x, C.y - Cm.y);
     const float2 Vbk = make_float2(C.y + Cm.y, Cm.x - C.x);
@@ -136,13 +137,11 @@ __device__ __forceinline__ float2 col_spectral(float2 C, float2 Cm, int k, int k
     const float2 Vbm = make_float2(Cm.y + C.y, C.x - Cm.x);
     float Xak = wk.x * Vak.x - wk.y * Vak.y, Xbk = wk.x * Vbk.x - wk.y * Vbk.y;
     float Xam = wm.x * Vam.x - wm.y * Vam.y, Xbm = wm.x * Vbm.x - wm.y * Vbm.y;
-    const float lak = (float)(2.0 * ck + 2.0 * ca - 4.0), lbk = (float)(2.0 * ck + 2.0 * cb - 4.0);
-    const float lam = (float)(2.0 * cm + 2.0 * ca - 4.0), lbm = (float)(2.0 * cm + 2.0 * cb - 4.0);
-    // X / lambda as X * (1/lambda) with a correctly rounded reciprocal
-    Xak = (k == 0 && ja0) ? 0.f : Xak * __frcp_rn(lak) * negs;
-    Xam = (km == 0 && ja0) ? 0.f : Xam * __frcp_rn(lam) * negs;
-    Xbk = hasb ? Xbk * __frcp_rn(lbk) * negs : 0.f;
-    Xbm = hasb ? Xbm * __frcp_rn(lbm) * negs : 0.f;
+    // X / lambda as X * (1/lambda) with a correctly rounded reciprocal (lambda = -(ck + ca))
+    Xak = (k == 0 && ja0) ? 0.f : Xak * __frcp_rn(-(ck + ca)) * negs;
+    Xam = (km == 0 && ja0) ? 0.f : Xam * __frcp_rn(-(cm + ca)) * negs;
+    Xbk = hasb ? Xbk * __frcp_rn(-(ck + cb)) * negs : 0.f;
+    Xbm = hasb ? Xbm * __frcp_rn(-(cm + cb)) * negs : 0.f;
     const float mak = k == 0 ? 0.f : Xam, mbk = k == 0 ? 0.f : Xbm;
     const float2 Pak = cmul(cconj(wk), make_float2(Xak, -mak));
     const float2 Pbk = cmul(cconj(wk), make_float2(Xbk, -mbk));

@@ -23,7 +23,7 @@
 
 // ============================================================ tables
 // Twiddles, DCT weights and Bluestein chirps in float64, rounded once.
-__global__ void k_tables(FftPlanDev f, DctPlanDev d, double* cosv, int Ncos) {
+__global__ void k_tables(FftPlanDev f, DctPlanDev d, float* sv, int Ncos) {
     float2* tw = const_cast<float2*>(f.tw);
     float2* dw = const_cast<float2*>(d.dctw);
     float2* ch = const_cast<float2*>(d.chirp);
@@ -43,9 +43,11 @@ __global__ void k_tables(FftPlanDev f, DctPlanDev d, double* cosv, int Ncos) {
             ch[k] = make_float2((float)c, (float)s);
         }
     }
-    // cos(pi*i/N) for the Neumann-Laplacian eigenvalues (utils_unwrap2d.py:1284-1289)
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Ncos; k += gridDim.x * blockDim.x)
-        cosv[k] = cospi((double)k / (double)Ncos);
+    // 4 sin^2(pi k / 2N) = 2 - 2 cos(pi k / N), eigenvalue part along this axis
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Ncos; k += gridDim.x * blockDim.x) {
+        const double sn = sinpi((double)k / (2.0 * (double)Ncos));
+        sv[k] = (float)(4.0 * sn * sn);
+    }
 }
 
 // Bluestein filter spectrum hspec = FFT_M(h) / M, h_j = chirp_|j| for |j| < N.
@@ -154,12 +156,14 @@ __global__ void __launch_bounds__(T) k_row_fwd(const GridDev* __restrict__ grids
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
-    const int i0 = 2 * local, i1 = i0 + 1;
-    const bool has1 = i1 < H;
     double acc[2] = {0.0, 0.0};
     float* U = (it & 1) ? G.U0 : G.U1;  // x of this IRLS iteration (U_nxt)
     const float* pk = (MODE == 2) ? ((cgk & 1) ? G.p1 : G.p0) : nullptr;
     const float alpha = (MODE == 2) ? st->alpha : 0.f;
+    for (int pair = local; pair < (H + 1) / 2; pair += nct) {
+    const int i0 = 2 * pair, i1 = i0 + 1;
+    const bool has1 = i1 < H;
+    __syncthreads();  // previous row pair's reads of sm are done
     for (int j = threadIdx.x; j < W; j += T) {
         const float a = rowfwd_value<MODE>(G, U, pk, alpha, i0, j, acc);
         const float b = has1 ? rowfwd_value<MODE>(G, U, pk, alpha, i1, j, acc) : 0.f;
@@ -177,6 +181,7 @@ __global__ void __launch_bounds__(T) k_row_fwd(const GridDev* __restrict__ grids
         const float2 w = __ldg(&dw[k]);
         G.T[(size_t)i0 * P + k] = w.x * Va.x - w.y * Va.y;
         if (has1) G.T[(size_t)i1 * P + k] = w.x * Vb.x - w.y * Vb.y;
+    }
     }
     if (MODE == 0 || MODE == 3) return;
     if (arrive<2>(G, local, nct, acc, red)) {
@@ -197,9 +202,13 @@ __global__ void __launch_bounds__(T) k_col(const GridDev* __restrict__ grids,
     const InstState* st = G.st;
     if (MODE == 1 && !(st->irls_active && st->cg_active)) return;
     const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
-    const int c0 = 2 * G.col_nseq * local;
+    const int nslab = (W + 2 * G.col_nseq - 1) / (2 * G.col_nseq);
+    for (int slab = local; slab < nslab; slab += nct) {
+    const int c0 = 2 * G.col_nseq * slab;
     const int nseq = min(G.col_nseq, (W - c0 + 1) >> 1);
+    __syncthreads();  // previous slab's reads of sm are done
     const DctPlanDev& PC = G.pcol;
     const int sd = PC.stride;
     float* __restrict__ Tm = G.T;
@@ -213,8 +222,8 @@ __global__ void __launch_bounds__(T) k_col(const GridDev* __restrict__ grids,
     __syncthreads();
     dft_n<T, EMAX>(sm, nseq, PC);
     const float2* __restrict__ dw = PC.dctw;
-    const double* __restrict__ cH = G.cosH;
-    const double* __restrict__ cW = G.cosW;
+    const float* __restrict__ sH = G.sH;
+    const float* __restrict__ sW = G.sW;
     const float negs = -1.0f / (4.0f * (float)H * (float)W);
     const int nh = H / 2 + 1;
     for (int q = threadIdx.x; q < nseq * nh; q += T) {
@@ -225,10 +234,10 @@ __global__ void __launch_bounds__(T) k_col(const GridDev* __restrict__ grids,
         const float2 C = base[k], Cm = base[km];
         const int ja = c0 + 2 * s;
         const bool hasb = ja + 1 < W;
-        const double ca = cW[ja], cb = hasb ? cW[ja + 1] : 1.0;
+        const float ca = sW[ja], cb = hasb ? sW[ja + 1] : 1.0f;
         const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
-        const float2 ok = col_spectral(C, Cm, k, km, wk, wm, cH[k], cH[km], ca, cb, ja == 0, hasb, negs);
-        if (km != k) base[km] = col_spectral(Cm, C, km, k, wm, wk, cH[km], cH[k], ca, cb, ja == 0, hasb, negs);
+        const float2 ok = col_spectral(C, Cm, k, km, wk, wm, sH[k], sH[km], ca, cb, ja == 0, hasb, negs);
+        if (km != k) base[km] = col_spectral(Cm, C, km, k, wm, wk, sH[km], sH[k], ca, cb, ja == 0, hasb, negs);
         base[k] = ok;
     }
     __syncthreads();
@@ -239,6 +248,7 @@ __global__ void __launch_bounds__(T) k_col(const GridDev* __restrict__ grids,
         const float2 v = sm[s * sd + mk_perm(i, H)];
         Tm[(size_t)i * P + c] = v.x;
         if (c + 1 < W) Tm[(size_t)i * P + c + 1] = -v.y;
+    }
     }
 }
 
@@ -257,8 +267,11 @@ __global__ void __launch_bounds__(T) k_row_inv(const GridDev* __restrict__ grids
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
-    const int i0 = 2 * local, i1 = i0 + 1;
+    double acc[2] = {0.0, 0.0};
+    for (int pair = local; pair < (H + 1) / 2; pair += nct) {
+    const int i0 = 2 * pair, i1 = i0 + 1;
     const bool has1 = i1 < H;
+    __syncthreads();  // previous row pair's reads of sm are done
     for (int k = threadIdx.x; k < W; k += T) {
         const float a = G.T[(size_t)i0 * P + k];
         const float b = has1 ? G.T[(size_t)i1 * P + k] : 0.f;
@@ -285,11 +298,11 @@ __global__ void __launch_bounds__(T) k_row_inv(const GridDev* __restrict__ grids
     }
     __syncthreads();
     dft_n<T, EMAX>(sm, 1, G.prow);
-    double acc[2] = {0.0, 0.0};
     for (int j = threadIdx.x; j < W; j += T) {
         const float2 v = sm[mk_perm(j, W)];
         rowinv_store<MODE>(G, i0, j, v.x, acc);
         if (has1) rowinv_store<MODE>(G, i1, j, -v.y, acc);
+    }
     }
     if (MODE == 3) return;
     if (arrive<2>(G, local, nct, acc, red)) {
@@ -345,15 +358,17 @@ __global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ g
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tx = local % G.sten_tiles_x, ty = local / G.sten_tiles_x;
-    const int j0 = tx * 128 + lane * 4;
-    const int i = ty * 16 + warp;
     const bool first = st->pfirst != 0;
     const float beta = st->beta;
     const float* __restrict__ z = G.z;
     const float* __restrict__ po = (k & 1) ? G.p0 : G.p1;
     float* __restrict__ pn = (k & 1) ? G.p1 : G.p0;
     double acc[1] = {0.0};
+    const int ntiles = G.sten_tiles_x * ((H + 15) / 16);
+    for (int tile = local; tile < ntiles; tile += nct) {
+    const int tx = tile % G.sten_tiles_x, ty = tile / G.sten_tiles_x;
+    const int j0 = tx * 128 + lane * 4;
+    const int i = ty * 16 + warp;
     // lanes past the last column load nothing (j0 < W implies j0 + 3 < P)
     const bool on = i < H && j0 < W;
     const bool hu = i > 0, hd = i < H - 1;
@@ -417,6 +432,7 @@ __global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ g
         }
         st4(pn, o, cur);
         st4(G.Ap, o, ap);
+    }
     }
     if (arrive<1>(G, local, nct, acc, red)) {
         finish_sum<1>(G, nct, acc, red);
@@ -708,13 +724,13 @@ cudaError_t unw_launch_col(int mode, int T, int emax, int nblk, size_t smem, cud
                      : launch_col_t<1>(T, emax, grid, smem, s, gd, starts, n);
 }
 
-cudaError_t unw_launch_tables(const FftPlanDev& f, const DctPlanDev& d, double* cosv, int Ncos,
+cudaError_t unw_launch_tables(const FftPlanDev& f, const DctPlanDev& d, float* sv, int Ncos,
                               cudaStream_t s) {
     int m = f.n > d.N ? f.n : d.N;
     m = m > Ncos ? m : Ncos;
     int nb = (m + 255) / 256;
     nb = nb > 64 ? 64 : nb;
-    k_tables<<<nb, 256, 0, s>>>(f, d, cosv, Ncos);
+    k_tables<<<nb, 256, 0, s>>>(f, d, sv, Ncos);
     return cudaGetLastError();
 }
 
