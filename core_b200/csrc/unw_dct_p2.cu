@@ -166,11 +166,18 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
     for (int c4 = t; c4 < N / 4; c4 += T) {
         const float4 ya = ld4f(Ta, 4 * c4);
         const float4 yb = has1 ? ld4f(Tb, 4 * c4) : make_float4(0.f, 0.f, 0.f, 0.f);
+        // mirrors N-k of k = 4c4..4c4+3: N-4c4 (.x of the chunk at N-4c4, none for
+        // c4 = 0) and N-4c4-1..N-4c4-3 (.w .z .y of the chunk at N-4c4-4)
+        const float4 za = ld4f(Ta, N - 4 * c4 - 4);
+        const float4 zb = has1 ? ld4f(Tb, N - 4 * c4 - 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float xa0 = c4 ? Ta[N - 4 * c4] : 0.f;
+        const float xb0 = (c4 && has1) ? Tb[N - 4 * c4] : 0.f;
+        const float ma[4] = {xa0, za.w, za.z, za.y};
+        const float mb[4] = {xb0, zb.w, zb.z, zb.y};
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             const int k = 4 * c4 + c;
-            const int km = (N - k) & (N - 1);
-            const float yam = k ? Ta[km] : 0.f, ybm = (k && has1) ? Tb[km] : 0.f;
+            const float yam = ma[c], ybm = mb[c];
             const float2 wc = cconj(__ldg(&dw[k]));
             const float2 Pa = cmul(wc, make_float2(f4get(ya, c), -yam));
             const float2 Pb = cmul(wc, make_float2(f4get(yb, c), -ybm));
@@ -224,16 +231,20 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
     const int ja = 2 * NSEQ * slab + 2 * s;
     const bool hasa = ja < W, hasb = ja + 1 < W;
     const bool vec = hasb && !(P & 1);
+    // FFT position m = t + T q reads source row 2m (q < 8) or 2N-1-2m (q >= 8):
+    // rows lo + q*step and hi - (q-8)*step with step = 2T rows
+    const size_t step = (size_t)(2 * T) * P;
+    float* const lo = Tm + (size_t)(2 * t) * P + ja;
+    float* const hi = Tm + (size_t)(N - 1 - 2 * t) * P + ja;
     __syncthreads();  // previous slab's reads of sm are done
 #pragma unroll
     for (int q = 0; q < 16; q++) {
-        const int m = t + T * q;
-        const size_t o = (size_t)mk_src<N>(m) * P + ja;
+        const float* a = q < 8 ? lo + q * step : hi - (q - 8) * step;
         float2 x = make_float2(0.f, 0.f);
-        if (vec) x = *reinterpret_cast<const float2*>(Tm + o);
-        else if (hasb) x = make_float2(Tm[o], Tm[o + 1]);
-        else if (hasa) x.x = Tm[o];
-        sms[pad16(m)] = x;
+        if (vec) x = *reinterpret_cast<const float2*>(a);
+        else if (hasb) x = make_float2(a[0], a[1]);
+        else if (hasa) x.x = a[0];
+        sms[pad16(t + T * q)] = x;
     }
     __syncthreads();
     smem_fft<N>(sms, t, tw);
@@ -251,12 +262,11 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
     smem_fft<N>(sms, t, tw);
 #pragma unroll
     for (int q = 0; q < 16; q++) {
-        const int m = t + T * q;
-        const size_t o = (size_t)mk_src<N>(m) * P + ja;
-        const float2 v = sms[pad16(m)];
-        if (vec) *reinterpret_cast<float2*>(Tm + o) = make_float2(v.x, -v.y);
-        else if (hasb) { Tm[o] = v.x; Tm[o + 1] = -v.y; }
-        else if (hasa) Tm[o] = v.x;
+        float* a = q < 8 ? lo + q * step : hi - (q - 8) * step;
+        const float2 v = sms[pad16(t + T * q)];
+        if (vec) *reinterpret_cast<float2*>(a) = make_float2(v.x, -v.y);
+        else if (hasb) { a[0] = v.x; a[1] = -v.y; }
+        else if (hasa) a[0] = v.x;
     }
     }
 }
@@ -295,9 +305,10 @@ static cudaError_t rowi_p2_n(int mode, int nblk, cudaStream_t s, const GridDev* 
     }
 }
 
-// column pairs per CTA: 512 threads and ~70 KB of shared memory up to N = 8192
+// column pairs per CTA: one sequence (N/16 threads) from N = 2048 up, so that
+// barriers span few warps and several CTAs share an SM; more for short columns
 template <int N>
-constexpr int col_nseq_p2() { return N >= 8192 ? 1 : (8192 / N > 8 ? 8 : 8192 / N); }
+constexpr int col_nseq_p2() { return N >= 2048 ? 1 : 2048 / N; }
 
 template <int N>
 static cudaError_t col_p2_n(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* st, int n) {
