@@ -55,9 +55,9 @@ constexpr int ELEM_MAX_CTAS = 1184;      // 8 x 148 SMs
 constexpr size_t COL_SMEM_BUDGET = 96 * 1024;
 constexpr int MAX_FFT = 16384;           // longest transform one CTA holds (1024 threads x 16)
 // CTAs of the persistent PCG kernels (148 SMs x resident CTAs per SM)
-constexpr int CTAS_ROW = 148 * 4;
-constexpr int CTAS_COL = 148 * 2;
-constexpr int CTAS_MATVEC = 148 * 2;
+constexpr int NUM_SMS = 148;
+constexpr int CTAS_ROW = NUM_SMS * 4;
+constexpr int CTAS_MATVEC = NUM_SMS * 2;
 
 size_t up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -271,7 +271,7 @@ int kind_ctas(const GridDev& G, int kind) {
     switch (kind) {
         // persistent kinds: at most a few CTAs per SM, each loops over its units
         case KS_ROWPAIR: return std::min((G.H + 1) / 2, CTAS_ROW);
-        case KS_COL: return std::min((G.W + 2 * G.col_nseq - 1) / (2 * G.col_nseq), CTAS_COL);
+        case KS_COL: return std::min((G.W + 2 * G.col_nseq - 1) / (2 * G.col_nseq), G.col_ctas);
         case KS_STEN: return G.sten_tiles_x * ((G.H + 8 * G.sten_rows - 1) / (8 * G.sten_rows));
         case KS_MATVEC: return std::min(G.sten_tiles_x * ((G.H + 15) / 16), CTAS_MATVEC);
         case KS_ELEM: return elem_ctas(npx);
@@ -446,6 +446,10 @@ int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbo
             S.sh.col_p2 = h;
             for (int g = 0; g < n; g++) S.hg[g].col_nseq = unw_p2_col_nseq(h);
         }
+        // persistent column pass: as many CTAs as fit on the SMs (<= 2048 threads, 4 CTAs)
+        const int cthreads = S.sh.col_p2 ? S.sh.col_p2 / 16 * unw_p2_col_nseq(S.sh.col_p2) : S.sh.col_T;
+        const int per_sm = std::max(1, std::min(4, 2048 / std::max(cthreads, 1)));
+        for (int g = 0; g < n; g++) S.hg[g].col_ctas = NUM_SMS * per_sm;
     }
     // CTA prefix arrays
     S.starts.assign((size_t)(KS_NKIND + 1) * (n + 1), 0);

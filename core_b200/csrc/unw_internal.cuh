@@ -85,6 +85,7 @@ struct GridDev {
     uint16_t* out_cc;    long long out_cc_pitch;
     int congruent;
     int col_nseq;               // complex sequences (column pairs) per column CTA
+    int col_ctas;               // CTA cap of the persistent column pass
     int sten_rows;              // rows per stencil CTA
     int sten_tiles_x;           // column tiles per stencil row strip
     float *gx, *gy, *wx, *wy;
