@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
     const size_t step = (size_t)(2 * T) * P;
     float* const lo = Tm + (size_t)(2 * t) * P + ja;
     float* const hi = Tm + (size_t)(N - 1 - 2 * t) * P + ja;
-    __syncthreads();  // previous slab's reads of sm are done
+    float2 v[16];
 #pragma unroll
     for (int q = 0; q < 16; q++) {
         const float* a = q < 8 ? lo + q * step : hi - (q - 8) * step;
@@ -244,29 +244,29 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
         if (vec) x = *reinterpret_cast<const float2*>(a);
         else if (hasb) x = make_float2(a[0], a[1]);
         else if (hasa) x.x = a[0];
-        sms[pad16(t + T * q)] = x;
+        v[q] = x;
     }
-    __syncthreads();
-    smem_fft<N>(sms, t, tw);
+    __syncthreads();  // previous slab's reads of sm are done
+    io_fft<N, true, false>(v, sms, t, tw);
     const float ca = hasa ? G.sW[ja] : 1.0f, cb = hasb ? G.sW[ja + 1] : 1.0f;
     for (int k = t; k <= N / 2; k += T) {
         const int km = (N - k) & (N - 1);
         const float2 C = sms[pad16(k)], Cm = sms[pad16(km)];
         const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
         const float ck = __ldg(&sH[k]), cm = __ldg(&sH[km]);
-        const float2 ok = col_spectral(C, Cm, k, km, wk, wm, ck, cm, ca, cb, ja == 0, hasb, negs);
-        if (km != k) sms[pad16(km)] = col_spectral(Cm, C, km, k, wm, wk, cm, ck, ca, cb, ja == 0, hasb, negs);
+        float2 ok, om;
+        col_spectral_pair(C, Cm, k, km, wk, wm, ck, cm, ca, cb, ja == 0, hasb, negs, ok, om);
+        if (km != k) sms[pad16(km)] = om;
         sms[pad16(k)] = ok;
     }
     __syncthreads();
-    smem_fft<N>(sms, t, tw);
+    io_fft<N, false, true>(v, sms, t, tw);
 #pragma unroll
     for (int q = 0; q < 16; q++) {
         float* a = q < 8 ? lo + q * step : hi - (q - 8) * step;
-        const float2 v = sms[pad16(t + T * q)];
-        if (vec) *reinterpret_cast<float2*>(a) = make_float2(v.x, -v.y);
-        else if (hasb) { a[0] = v.x; a[1] = -v.y; }
-        else if (hasa) a[0] = v.x;
+        if (vec) *reinterpret_cast<float2*>(a) = make_float2(v[q].x, -v[q].y);
+        else if (hasb) { a[0] = v[q].x; a[1] = -v[q].y; }
+        else if (hasa) a[0] = v[q].x;
     }
     }
 }
@@ -305,10 +305,9 @@ static cudaError_t rowi_p2_n(int mode, int nblk, cudaStream_t s, const GridDev* 
     }
 }
 
-// column pairs per CTA: one sequence (N/16 threads) from N = 2048 up, so that
-// barriers span few warps and several CTAs share an SM; more for short columns
+// column pairs per CTA: 512 threads (two pairs at N = 4096: 16-byte row segments)
 template <int N>
-constexpr int col_nseq_p2() { return N >= 2048 ? 1 : 2048 / N; }
+constexpr int col_nseq_p2() { return N >= 8192 ? 1 : (8192 / N > 8 ? 8 : 8192 / N); }
 
 template <int N>
 static cudaError_t col_p2_n(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* st, int n) {

@@ -122,6 +122,22 @@ __device__ __forceinline__ void smem_fft_rec(float2* sm, int t, const float2* tw
     }
 }
 
+template <int N, int P, int NS, bool IN_REG, bool OUT_REG>
+__device__ __forceinline__ void io_fft_rec(float2 (&v)[16], float2* sm, int t, const float2* tw) {
+    if constexpr (P < RegFft<N>::NPASS) {
+        constexpr int R = (P < RegFft<N>::NP16) ? 16 : (1 << RegFft<N>::REM);
+        reg_pass<N, R, NS, IN_REG && P == 0, OUT_REG && P == RegFft<N>::NPASS - 1>(v, sm, t, tw);
+        io_fft_rec<N, P + 1, NS * R, IN_REG, OUT_REG>(v, sm, t, tw);
+    }
+}
+
+// Forward FFT with the input in registers (stride-T layout) or in shared memory
+// (natural order), and the output likewise; the other side goes through `sm`.
+template <int N, bool IN_REG, bool OUT_REG>
+__device__ __forceinline__ void io_fft(float2 (&v)[16], float2* sm, int t, const float2* tw) {
+    io_fft_rec<N, 0, 1, IN_REG, OUT_REG>(v, sm, t, tw);
+}
+
 // Forward FFT of the sequence held in shared memory (natural order, padded
 // addresses pad16(i)), result in place.  Registers are used only inside each
 // pass.  The caller synchronises before the call (inputs written) and the

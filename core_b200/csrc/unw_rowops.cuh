@@ -122,6 +122,33 @@ __device__ __forceinline__ void rowinv_finalize(InstState* st, const double (&ac
     }
 }
 
+// Both outputs of the column-pass spectral step for the frequency pair
+// (k, km = H-k): the DCT-II extraction and the eigenvalue scaling are shared,
+// only the DCT-III pre-twiddles differ.  For k = 0 (km = 0) or k = km the
+// second output equals the first and is not used.
+__device__ __forceinline__ void col_spectral_pair(float2 C, float2 Cm, int k, int km, float2 wk, float2 wm,
+                                                  float ck, float cm, float ca, float cb, bool ja0, bool hasb,
+                                                  float negs, float2& ok, float2& om) {
+    const float2 Vak = make_float2(C.x + Cm.x, C.y - Cm.y);
+    const float2 Vbk = make_float2(C.y + Cm.y, Cm.x - C.x);
+    const float2 Vam = make_float2(Vak.x, -Vak.y);   // conj: the pair's extraction is symmetric
+    const float2 Vbm = make_float2(Vbk.x, -Vbk.y);
+    float Xak = wk.x * Vak.x - wk.y * Vak.y, Xbk = wk.x * Vbk.x - wk.y * Vbk.y;
+    float Xam = wm.x * Vam.x - wm.y * Vam.y, Xbm = wm.x * Vbm.x - wm.y * Vbm.y;
+    Xak = (k == 0 && ja0) ? 0.f : Xak * __frcp_rn(-(ck + ca)) * negs;
+    Xam = (km == 0 && ja0) ? 0.f : Xam * __frcp_rn(-(cm + ca)) * negs;
+    Xbk = hasb ? Xbk * __frcp_rn(-(ck + cb)) * negs : 0.f;
+    Xbm = hasb ? Xbm * __frcp_rn(-(cm + cb)) * negs : 0.f;
+    // DCT-III pre-twiddle V'_k = conj(w_k) (Y_k - i Y_{H-k}) with Y_H = 0
+    const float mak = k == 0 ? 0.f : Xam, mbk = k == 0 ? 0.f : Xbm;
+    const float2 Pak = cmul(cconj(wk), make_float2(Xak, -mak));
+    const float2 Pbk = cmul(cconj(wk), make_float2(Xbk, -mbk));
+    ok = cconj(make_float2(Pak.x - Pbk.y, Pak.y + Pbk.x));
+    const float2 Pam = cmul(cconj(wm), make_float2(Xam, -Xak));
+    const float2 Pbm = cmul(cconj(wm), make_float2(Xbm, -Xbk));
+    om = cconj(make_float2(Pam.x - Pbm.y, Pam.y + Pbm.x));
+}
+
 // Column-pass spectral step for one frequency pair (k, H-k) of two columns
 // (ja, ja+1) whose DFT outputs are C = C_k and Cm = C_{H-k}: DCT-II extraction,
 // division by the Neumann-Laplacian eigenvalue lambda = -(sH + sW) (see
