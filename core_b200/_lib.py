@@ -80,6 +80,7 @@ SIGNATURES = {
                                       C.c_void_p, C.c_size_t, C.c_void_p]),
     "unw_apply_preconditioner": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
                                            C.c_size_t, C.c_void_p]),
+    "unw_apply_preconditioner_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
 }
 
 _lock = threading.Lock()

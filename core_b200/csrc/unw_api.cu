@@ -21,15 +21,13 @@
 
 namespace {
 
-thread_local std::string g_err;
+thread_local char g_err[512];
 
 int set_err(int code, const char* fmt, ...) {
-    char buf[512];
     va_list ap;
     va_start(ap, fmt);
-    vsnprintf(buf, sizeof(buf), fmt, ap);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
     va_end(ap);
-    g_err = buf;
     return code;
 }
 
@@ -656,12 +654,15 @@ int op_upload(Solver& S) {
 
 }  // namespace
 
+// error text setter shared with the other host translation units
+int unw_set_error(int code, const char* msg) { return set_err(code, "%s", msg); }
+
 // ================================================================== C ABI
 extern "C" {
 
 int unw_abi_version(void) { return UNW_ABI_VERSION; }
 
-const char* unw_last_error(void) { return g_err.c_str(); }
+const char* unw_last_error(void) { return g_err; }
 
 size_t unw_batch_workspace_bytes(int32_t n, const int64_t* H, const int64_t* W) {
     if (n <= 0 || !H || !W) return 0;

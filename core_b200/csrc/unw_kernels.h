@@ -24,6 +24,9 @@ enum {
     UNW_K_LAP_APPLY
 };
 
+// records the thread-local error text returned by unw_last_error(); returns code
+int unw_set_error(int code, const char* msg);
+
 // solver kernels
 cudaError_t unw_launch_tables(const FftPlanDev& f, const DctPlanDev& d, float* sv, int Ncos,
                               cudaStream_t s);

@@ -154,6 +154,22 @@ UNW_API int unw_apply_laplacian(const float* x, const float* wx, const float* wy
 UNW_API int unw_apply_preconditioner(const float* r, int64_t H, int64_t W, float* z,
                              void* workspace, size_t workspace_bytes, void* cuda_stream);
 
+/*
+ * Allocation-free variant of unw_apply_preconditioner.  It has no counterpart
+ * in the reference.  It is for callers that cannot allocate device memory
+ * where they need the operator (inside another framework's graph capture or
+ * stream-ordered region, allocation-free real-time loops, C callers without
+ * an allocator): its scratch is one 16 MiB device array that the library
+ * holds on every GPU that loads it, so the caller passes only r and z (dense,
+ * pitch W, device pointers).  Limit: H * W <= 3932160 and transform lengths
+ * <= 16384, otherwise UNW_E_UNSUPPORTED.  All calls on a device share the
+ * array: calls that overlap on the GPU race (order them on one stream).  The
+ * first call on a device looks up the array's address; make it before any
+ * stream capture.
+ */
+UNW_API int unw_apply_preconditioner_noalloc(const float* r, int64_t H, int64_t W, float* z,
+                                             void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
