@@ -8,6 +8,8 @@
 // layout is computed by one function for both sizing and carving.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <array>
+#include <map>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -182,7 +184,7 @@ BatchLayout batch_layout(int n, const long long* H, const long long* W) {
     B.colany = take(sizeof(int) * (size_t)std::max(1LL, sw));
     B.bbox = take(sizeof(int) * 4 * (size_t)n);
     B.gdev = take(sizeof(GridDev) * (size_t)n);
-    B.starts = take(sizeof(int) * (size_t)KS_NKIND * (n + 1) + sizeof(int) * (n + 1));
+    B.starts = take(sizeof(int) * (size_t)(KS_NKIND + 1) * (2 * (size_t)n + 1));
     for (int g = 0; g < n; g++) {
         GridLayout L = grid_layout(H[g], W[g]);
         B.base.push_back(o);
@@ -329,12 +331,36 @@ int validate_params(const unw_params* p) {
     return UNW_OK;
 }
 
+// column pairs per generic column CTA under the shared-memory budget
+int col_nseq_generic(int nfft, int W) {
+    int nseq = (int)std::max<size_t>(1, std::min<size_t>(8, COL_SMEM_BUDGET / ((size_t)nfft * sizeof(float2))));
+    return std::min(nseq, (W + 1) / 2);
+}
+
+// Launch-group key of a cropped H x W grid: grids with equal keys share every
+// kernel configuration (power-of-two length, or generic thread count) per axis.
+std::array<int, 4> group_key(int H, int W) {
+    if (H <= 0 || W <= 0) return {-1, 0, -1, 0};
+    auto p2 = [](int n) { return n >= 256 && n <= MAX_FFT && (n & (n - 1)) == 0; };
+    std::array<int, 4> k{};
+    if (p2(W)) { k[0] = 1; k[1] = W; }
+    else { const HostPlan hp = make_plan(W); k[0] = 0; k[1] = pick_threads(hp.n, hp.cap); }
+    if (p2(H)) { k[2] = 1; k[3] = H; }
+    else {
+        const HostPlan hp = make_plan(H);
+        int nseq = col_nseq_generic(hp.n, W), cT = 0;
+        while (nseq >= 1 && !(cT = pick_threads((long long)nseq * hp.n, hp.cap))) nseq--;
+        k[2] = 0; k[3] = cT;
+    }
+    return k;
+}
+
 // Per-grid descriptors, FFT plans, launch shapes, CTA prefix arrays and
 // tables for grids cropped to bbox (r0, r1, c0, c1 per grid).
-int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbox, const unw_params* prm,
-            char* base, const BatchLayout& B, cudaStream_t s, bool dense) {
-    const std::vector<long long> H0 = [&] { std::vector<long long> v(n); for (int g = 0; g < n; g++) v[g] = grids[g].H; return v; }();
-    const std::vector<long long> W0 = [&] { std::vector<long long> v(n); for (int g = 0; g < n; g++) v[g] = grids[g].W; return v; }();
+int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const std::vector<int>& bbox,
+            const unw_params* prm, char* base, const BatchLayout& B, cudaStream_t s, bool dense, int slot,
+            int soff) {
+    const int n = (int)idx.size();
     S.n = n;
     S.s = s;
     S.hg.resize(n);
@@ -345,15 +371,16 @@ int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbo
     S.sc.eps2 = (float)((double)prm->epsilon * (double)prm->epsilon);
     S.sc.conncomp_size = prm->conncomp_size;
     std::vector<HostPlan> prow(n), pcol(n);
-    for (int g = 0; g < n; g++) {
+    for (int gi = 0; gi < n; gi++) {
+        const int g = idx[gi];
         const unw_grid& q = grids[g];
         const GridLayout& L = B.g[g];
         char* gb = base + B.base[g];
-        GridDev& G = S.hg[g];
+        GridDev& G = S.hg[gi];
         memset(&G, 0, sizeof(G));
         const int r0 = bbox[4 * g], r1 = bbox[4 * g + 1], c0 = bbox[4 * g + 2], c1 = bbox[4 * g + 3];
-        G.H0 = (int)H0[g];
-        G.W0 = (int)W0[g];
+        G.H0 = (int)q.H;
+        G.W0 = (int)q.W;
         G.H = r1 - r0;
         G.W = c1 - c0;
         G.r0 = r0;
@@ -389,9 +416,9 @@ int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbo
         G.lab_cap = (int)std::min<long long>(L.lab_cap, (long long)G.H * G.W / 2 + 2);
         G.ntiles = (int)(((long long)G.H * G.W + 4095) / 4096);
         if (G.H == 0) continue;
-        prow[g] = make_plan(G.W);
-        pcol[g] = make_plan(G.H);
-        const HostPlan* pl[2] = {&prow[g], &pcol[g]};
+        prow[gi] = make_plan(G.W);
+        pcol[gi] = make_plan(G.H);
+        const HostPlan* pl[2] = {&prow[gi], &pcol[gi]};
         DctPlanDev* dp[2] = {&G.prow, &G.pcol};
         size_t tw[2] = {L.tw_r, L.tw_c}, hs[2] = {L.hs_r, L.hs_c}, dw[2] = {L.dw_r, L.dw_c},
                ch[2] = {L.ch_r, L.ch_c};
@@ -414,18 +441,17 @@ int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbo
             D.hspec = (const float2*)(gb + hs[d]);
         }
         // row kernel: one complex sequence (two rows) of fft_len(W)
-        const int rT = pick_threads(prow[g].n, prow[g].cap);
+        const int rT = pick_threads(prow[gi].n, prow[gi].cap);
         // column kernel: nseq column pairs of fft_len(H) under the shared-memory budget
-        int nseq = (int)std::max<size_t>(1, std::min<size_t>(8, COL_SMEM_BUDGET / ((size_t)pcol[g].n * sizeof(float2))));
-        nseq = std::min(nseq, (G.W + 1) / 2);
+        int nseq = col_nseq_generic(pcol[gi].n, G.W);
         int cT = 0;
-        while (nseq >= 1 && !(cT = pick_threads((long long)nseq * pcol[g].n, pcol[g].cap))) nseq--;
+        while (nseq >= 1 && !(cT = pick_threads((long long)nseq * pcol[gi].n, pcol[gi].cap))) nseq--;
         if (!rT || !cT) return set_err(UNW_E_UNSUPPORTED, "grid %d: no launch shape", g);
         G.col_nseq = nseq;
         S.sh.row_T = std::max(S.sh.row_T, rT);
         S.sh.col_T = std::max(S.sh.col_T, cT);
-        S.sh.row_smem = std::max(S.sh.row_smem, (size_t)prow[g].n * sizeof(float2));
-        S.sh.col_smem = std::max(S.sh.col_smem, (size_t)nseq * pcol[g].n * sizeof(float2));
+        S.sh.row_smem = std::max(S.sh.row_smem, (size_t)prow[gi].n * sizeof(float2));
+        S.sh.col_smem = std::max(S.sh.col_smem, (size_t)nseq * pcol[gi].n * sizeof(float2));
         G.sten_tiles_x = (G.W + 127) / 128;
         G.sten_rows = 1;
     }
@@ -461,8 +487,8 @@ int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbo
         S.starts[(size_t)k * (n + 1) + n] = acc;
         S.total[k] = acc;
     }
-    S.dg = (GridDev*)(base + B.gdev);
-    S.dstarts = (int*)(base + B.starts);
+    S.dg = (GridDev*)(base + B.gdev) + slot;
+    S.dstarts = (int*)(base + B.starts) + soff;
     CK(cudaMemcpyAsync(S.dg, S.hg.data(), sizeof(GridDev) * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(S.dstarts, S.starts.data(), sizeof(int) * S.starts.size(), cudaMemcpyHostToDevice, s));
 
@@ -480,50 +506,16 @@ int prepare(Solver& S, int n, const unw_grid* grids, const std::vector<int>& bbo
     return UNW_OK;
 }
 
-// ------------------------------------------------------------ batch solve
-int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, size_t ws_bytes,
-                unw_stats* stats, cudaStream_t s) {
-    if (n <= 0 || !grids) return set_err(UNW_E_ARG, "empty batch");
-    int rc = validate_params(prm);
-    if (rc) return rc;
-    std::vector<long long> H0(n), W0(n);
-    for (int g = 0; g < n; g++) {
-        const unw_grid& q = grids[g];
-        if (!q.phase || !q.out_u || !q.out_cc) return set_err(UNW_E_ARG, "grid %d: null pointer", g);
-        if (q.H <= 0 || q.W <= 0) return set_err(UNW_E_ARG, "grid %d: bad shape %lld x %lld", g, q.H, q.W);
-        if (q.H * q.W >= (1LL << 31)) return set_err(UNW_E_UNSUPPORTED, "grid %d: too many pixels", g);
-        if (q.phase_pitch < q.W || q.out_u_pitch < q.W || q.out_cc_pitch < q.W ||
-            (q.weight && q.weight_pitch < q.W))
-            return set_err(UNW_E_ARG, "grid %d: pitch smaller than width", g);
-        H0[g] = q.H;
-        W0[g] = q.W;
-    }
-    BatchLayout B = batch_layout(n, H0.data(), W0.data());
-    if (!ws) return set_err(UNW_E_ARG, "workspace is NULL");
-    char* base = (char*)up((size_t)ws, ALIGN);
-    if ((size_t)(base - (char*)ws) + B.total - ALIGN > ws_bytes)
-        return set_err(UNW_E_WORKSPACE, "workspace %zu bytes < %zu needed", ws_bytes, B.total);
-
-    // 1. bounding boxes
-    int* rowany = (int*)(base + B.rowany);
-    int* colany = (int*)(base + B.colany);
-    int* dbbox = (int*)(base + B.bbox);
-    {
-        long long ro = 0, co = 0;
-        for (int g = 0; g < n; g++) {
-            CK(unw_launch_bbox(grids[g].phase, grids[g].phase_pitch, (int)H0[g], (int)W0[g], rowany + ro,
-                               colany + co, dbbox + 4 * g, s));
-            ro += H0[g];
-            co += W0[g];
-        }
-    }
-    std::vector<int> bbox(4 * n);
-    CK(cudaMemcpyAsync(bbox.data(), dbbox, sizeof(int) * 4 * n, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-
+// One launch group: every kernel covers the group's grids with shapes sized for
+// them; each grid stops on its own convergence test.
+int solve_group(const std::vector<int>& idx, const unw_grid* grids, const std::vector<int>& bbox,
+                const unw_params* prm, char* base, const BatchLayout& B, unw_stats* stats, cudaStream_t s,
+                int slot, int soff) {
+    const int n = (int)idx.size();
+    int rc;
     Solver S;
     S.prof.on = (prm->flags & UNW_F_PROFILE) != 0;
-    rc = prepare(S, n, grids, bbox, prm, base, B, s, false);
+    rc = prepare(S, idx, grids, bbox, prm, base, B, s, false, slot, soff);
     if (rc) return rc;
 
     // 4. setup and DCT initial solve (utils_unwrap2d.py:1228-1513)
@@ -582,9 +574,9 @@ int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, s
             for (int L : order)
                 if (cnt[L] >= prm->conncomp_size) remap[L] = nw++;
             if (nw - 1 > 65535)
-                return set_err(UNW_E_OVERFLOW, "grid %d: %d components do not fit uint16 labels", g, nw - 1);
+                return set_err(UNW_E_OVERFLOW, "grid %d: %d components do not fit uint16 labels", idx[g], nw - 1);
             CK(cudaMemcpyAsync(G.remap, remap.data(), sizeof(int) * (nl + 1), cudaMemcpyHostToDevice, s));
-            if (stats) stats[g].n_components = nw - 1;
+            if (stats) stats[idx[g]].n_components = nw - 1;
         }
         PL(UNW_PROF_POST, unw_launch_post(UNW_P_WRITE, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
     }
@@ -601,19 +593,20 @@ int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, s
         else {
             status = st.status;
             if (st.n_nonfinite) { status |= UNW_S_NONFINITE_OUT; ret = UNW_W_NUMERIC; }
-            else if (!st.hist_ok) return set_err(UNW_E_UNSUPPORTED, "grid %d: post-processing limits exceeded", g);
+            else if (!st.hist_ok) return set_err(UNW_E_UNSUPPORTED, "grid %d: post-processing limits exceeded", idx[g]);
         }
         if (stats) {
-            unw_stats& o = stats[g];
-            const int ncomp = o.n_components;
-            memset(&o, 0, sizeof(o));
-            o.n_components = (G.H > 0 && !st.n_nonfinite) ? ncomp : 0;
+            // stats were zeroed by solve_batch; n_components was set by the relabel
+            // step, the profile sums (grid 0) accumulate over groups
+            unw_stats& o = stats[idx[g]];
+            if (!(G.H > 0 && !st.n_nonfinite)) o.n_components = 0;
             o.irls_iters = G.H ? st.irls_iter : 0;
             o.cg_iters_total = G.H ? st.cg_total : 0;
             o.cg_iters_last = (G.H && st.irls_iter > 0 && st.irls_iter <= UNW_MAX_LOG) ? st.cg_log[st.irls_iter - 1] : 0;
             o.n_labels = G.H ? st.n_labels : 0;
             o.status = status;
-            o.bbox[0] = bbox[4 * g]; o.bbox[1] = bbox[4 * g + 1]; o.bbox[2] = bbox[4 * g + 2]; o.bbox[3] = bbox[4 * g + 3];
+            const int og = idx[g];
+            o.bbox[0] = bbox[4 * og]; o.bbox[1] = bbox[4 * og + 1]; o.bbox[2] = bbox[4 * og + 2]; o.bbox[3] = bbox[4 * og + 3];
             o.rel_change = st.rel_change;
             o.best_residual = st.best_residual;
             o.k_median = st.kmed;
@@ -621,6 +614,64 @@ int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, s
         }
     }
     if (stats && S.prof.on) S.prof.collect(stats[0].prof_ms, stats[0].prof_launches);
+    return ret;
+}
+
+// ------------------------------------------------------------ batch solve
+int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, size_t ws_bytes,
+                unw_stats* stats, cudaStream_t s) {
+    if (n <= 0 || !grids) return set_err(UNW_E_ARG, "empty batch");
+    int rc = validate_params(prm);
+    if (rc) return rc;
+    std::vector<long long> H0(n), W0(n);
+    for (int g = 0; g < n; g++) {
+        const unw_grid& q = grids[g];
+        if (!q.phase || !q.out_u || !q.out_cc) return set_err(UNW_E_ARG, "grid %d: null pointer", g);
+        if (q.H <= 0 || q.W <= 0) return set_err(UNW_E_ARG, "grid %d: bad shape %lld x %lld", g, q.H, q.W);
+        if (q.H * q.W >= (1LL << 31)) return set_err(UNW_E_UNSUPPORTED, "grid %d: too many pixels", g);
+        if (q.phase_pitch < q.W || q.out_u_pitch < q.W || q.out_cc_pitch < q.W ||
+            (q.weight && q.weight_pitch < q.W))
+            return set_err(UNW_E_ARG, "grid %d: pitch smaller than width", g);
+        H0[g] = q.H;
+        W0[g] = q.W;
+    }
+    BatchLayout B = batch_layout(n, H0.data(), W0.data());
+    if (!ws) return set_err(UNW_E_ARG, "workspace is NULL");
+    char* base = (char*)up((size_t)ws, ALIGN);
+    if ((size_t)(base - (char*)ws) + B.total - ALIGN > ws_bytes)
+        return set_err(UNW_E_WORKSPACE, "workspace %zu bytes < %zu needed", ws_bytes, B.total);
+
+    // 1. bounding boxes
+    int* rowany = (int*)(base + B.rowany);
+    int* colany = (int*)(base + B.colany);
+    int* dbbox = (int*)(base + B.bbox);
+    {
+        long long ro = 0, co = 0;
+        for (int g = 0; g < n; g++) {
+            CK(unw_launch_bbox(grids[g].phase, grids[g].phase_pitch, (int)H0[g], (int)W0[g], rowany + ro,
+                               colany + co, dbbox + 4 * g, s));
+            ro += H0[g];
+            co += W0[g];
+        }
+    }
+    std::vector<int> bbox(4 * n);
+    CK(cudaMemcpyAsync(bbox.data(), dbbox, sizeof(int) * 4 * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+
+    // 2. launch groups (kernel configuration per axis), solved one after another
+    std::map<std::array<int, 4>, std::vector<int>> groups;
+    for (int g = 0; g < n; g++)
+        groups[group_key(bbox[4 * g + 1] - bbox[4 * g], bbox[4 * g + 3] - bbox[4 * g + 2])].push_back(g);
+    if (stats)
+        for (int g = 0; g < n; g++) memset(&stats[g], 0, sizeof(unw_stats));
+    int ret = UNW_OK, slot = 0, soff = 0;
+    for (auto& kv : groups) {
+        rc = solve_group(kv.second, grids, bbox, prm, base, B, stats, s, slot, soff);
+        if (rc < 0) return rc;
+        if (rc == UNW_W_NUMERIC) ret = rc;
+        slot += (int)kv.second.size();
+        soff += (KS_NKIND + 1) * ((int)kv.second.size() + 1);
+    }
     return ret;
 }
 
@@ -644,7 +695,7 @@ int op_prepare(Solver& S, int64_t H, int64_t W, void* ws, size_t wsb, cudaStream
     unw_params prm{};
     prm.epsilon = 1e-2f;
     std::vector<int> bbox = {0, (int)H, 0, (int)W};
-    return prepare(S, 1, &q, bbox, &prm, base, B, s, true);
+    return prepare(S, std::vector<int>{0}, &q, bbox, &prm, base, B, s, true, 0, 0);
 }
 
 int op_upload(Solver& S) {
