@@ -161,6 +161,14 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
     const bool has1 = i1 < H;
     const float* __restrict__ Ta = G.T + (size_t)i0 * P;
     const float* __restrict__ Tb = G.T + (size_t)i1 * P;
+    if (MODE == 1 || MODE == 2) {
+        // the epilogue reads r of these rows after the FFT: start them towards L2 now
+        const float* ra = G.r + (size_t)i0 * P;
+        for (int c = t * 32; c < N; c += T * 32) {
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(ra + c));
+            if (has1) asm volatile("prefetch.global.L2 [%0];" ::"l"(ra + P + c));
+        }
+    }
     __syncthreads();  // previous row pair's reads of sm are done
     // DCT-III pre-twiddle: V'_k = conj(w_k) (Y_k - i Y_{N-k}), Y_N = 0; store conj(C')
     for (int c4 = t; c4 < N / 4; c4 += T) {
