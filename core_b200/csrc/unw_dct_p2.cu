@@ -48,6 +48,34 @@ __device__ __forceinline__ float4 rowf_vals4(const GridDev& G, float* __restrict
         return rn;
     } else if (MODE == 3) {
         return ld4f(G.r, o);
+    } else if (MODE == 1) {
+        // r = b - A x at columns j..j+3 (x = U), A in the reference's op order
+        const int H = G.H, W = G.W, P = G.P;
+        const float4 x4 = ld4f(U, o), b4 = ld4f(G.b, o), wx4 = ld4f(G.wIx, o), wy4 = ld4f(G.wIy, o);
+        const float4 xu4 = i > 0 ? ld4f(U, o - P) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 wyu4 = i > 0 ? ld4f(G.wIy, o - P) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 xd4 = i < H - 1 ? ld4f(U, o + P) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float xl = j > 0 ? U[o - 1] : 0.f, wxl = j > 0 ? G.wIx[o - 1] : 0.f;
+        const float xr = j + 4 < W ? U[o + 4] : 0.f;
+        const float xs[6] = {xl, x4.x, x4.y, x4.z, x4.w, xr};
+        const float wxs[5] = {wxl, wx4.x, wx4.y, wx4.z, wx4.w};
+        float out[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int jj = j + q;
+            const float xc = xs[q + 1];
+            float res = 0.f;
+            if (jj > 0) res = fsub(res, fmul(fsub(xc, xs[q]), wxs[q]));
+            if (jj < W - 1) res = fadd(res, fmul(fsub(xs[q + 2], xc), wxs[q + 1]));
+            if (i > 0) res = fsub(res, fmul(fsub(xc, f4get(xu4, q)), f4get(wyu4, q)));
+            if (i < H - 1) res = fadd(res, fmul(fsub(f4get(xd4, q), xc), f4get(wy4, q)));
+            const float val = fsub(f4get(b4, q), -res);
+            out[q] = val;
+            acc[0] += isfinite(val) ? 0.0 : 1.0;
+        }
+        const float4 r4 = make_float4(out[0], out[1], out[2], out[3]);
+        st4f(G.r, o, r4);
+        return r4;
     } else {
         float4 v;
         v.x = rowfwd_value<MODE>(G, U, pk, alpha, i, j, acc);

@@ -455,6 +455,9 @@ __global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ g
 // IRLS head (utils_unwrap2d.py:1536-1581): recentre, residual gradients,
 // best-iterate test, IRLS weights and right-hand side.  Reads U_cur, writes
 // the recentred iterate to U_nxt (U_cur keeps u_prev for the convergence test).
+// One warp per row, 4 columns per lane; the weight of the left edge comes from
+// the neighbouring lane, the weight of the upper edge is recomputed from the
+// row above (the same float32 operations, so it equals that row's own value).
 __device__ __forceinline__ float irls_w(float w, float r, float eps2) {
     return clampf_nan(fdiv(w, __fsqrt_rn(fadd(fmul(r, r), eps2))), 1e-6f, 1e6f);
 }
@@ -472,41 +475,77 @@ __global__ void __launch_bounds__(256) k_head(const GridDev* __restrict__ grids,
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tx = local % G.sten_tiles_x, ty = local / G.sten_tiles_x;
     const int j0 = tx * 128 + lane * 4;
-    const int ib = (ty * 8 + warp) * G.sten_rows, ie = min(H, ib + G.sten_rows);
+    const int i = ty * 8 + warp;
     const float m = st->vcount > 0 ? (float)st->mean : 0.f;
     const float eps2 = st->eps2;
     const float* __restrict__ uc = (it & 1) ? G.U1 : G.U0;
     float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
     double acc[2] = {0.0, 0.0};
-    for (int i = ib; i < ie; i++) {
-        for (int c = 0; c < 4; c++) {
-            const int j = j0 + c;
-            if (j >= W) break;
-            const size_t o = (size_t)i * P + j;
-            const float cv = fsub(uc[o], m);
-            // residual gradients r = grad(u) - g (last column/row: 0 - g)
-            const float rx = (j < W - 1) ? fsub(fsub(fsub(uc[o + 1], m), cv), G.gx[o]) : fsub(0.f, G.gx[o]);
-            const float ry = (i < H - 1) ? fsub(fsub(fsub(uc[o + P], m), cv), G.gy[o]) : fsub(0.f, G.gy[o]);
-            acc[0] += (double)fmul(rx, rx) + (double)fmul(ry, ry);
-            acc[1] += isfinite(cv) ? 0.0 : 1.0;
-            const float wix = irls_w(G.wx[o], rx, eps2);
-            const float wiy = irls_w(G.wy[o], ry, eps2);
-            float bv = 0.f;
-            if (j > 0) {
-                const float rxl = fsub(fsub(cv, fsub(uc[o - 1], m)), G.gx[o - 1]);
-                bv = fadd(bv, fmul(irls_w(G.wx[o - 1], rxl, eps2), G.gx[o - 1]));
-            }
-            if (j < W - 1) bv = fsub(bv, fmul(wix, G.gx[o]));
-            if (i > 0) {
-                const float ryu = fsub(fsub(cv, fsub(uc[o - P], m)), G.gy[o - P]);
-                bv = fadd(bv, fmul(irls_w(G.wy[o - P], ryu, eps2), G.gy[o - P]));
-            }
-            if (i < H - 1) bv = fsub(bv, fmul(wiy, G.gy[o]));
-            un[o] = cv;
-            G.wIx[o] = wix;
-            G.wIy[o] = wiy;
-            G.b[o] = bv;
+    const bool on = i < H && j0 < W;
+    const bool hu = i > 0, hd = i < H - 1;
+    const size_t o = (size_t)i * P + j0;
+    F4 u{}, ud{}, uu{}, gx{}, gy{}, gyu{}, wx{}, wy{}, wyu{};
+    float ul = 0.f, ur = 0.f, gxl = 0.f, wxl = 0.f;
+    if (on) {
+        u = ld4(uc, o);
+        if (hd) ud = ld4(uc, o + P);
+        if (hu) { uu = ld4(uc, o - P); gyu = ld4(G.gy, o - P); wyu = ld4(G.wy, o - P); }
+        gx = ld4(G.gx, o);
+        gy = ld4(G.gy, o);
+        wx = ld4(G.wx, o);
+        wy = ld4(G.wy, o);
+        if (lane == 0 && j0 > 0) { ul = uc[o - 1]; gxl = G.gx[o - 1]; wxl = G.wx[o - 1]; }
+        if (lane == 31 && j0 + 4 < W) ur = uc[o + 4];
+    }
+    F4 c, rx, ry, wix, wiy, bv;
+#pragma unroll
+    for (int q = 0; q < 4; q++) c.v[q] = fsub(u.v[q], m);
+    // right neighbour of column j0+3 and left neighbour of j0 (recentred)
+    float cr = __shfl_down_sync(0xffffffffu, c.v[0], 1);
+    if (lane == 31) cr = fsub(ur, m);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int j = j0 + q;
+        const float right = q == 3 ? cr : c.v[q + 1];
+        // r = grad(u) - g, last column / row: 0 - g
+        rx.v[q] = (j < W - 1) ? fsub(fsub(right, c.v[q]), gx.v[q]) : fsub(0.f, gx.v[q]);
+        ry.v[q] = hd ? fsub(fsub(fsub(ud.v[q], m), c.v[q]), gy.v[q]) : fsub(0.f, gy.v[q]);
+        wix.v[q] = irls_w(wx.v[q], rx.v[q], eps2);
+        wiy.v[q] = irls_w(wy.v[q], ry.v[q], eps2);
+    }
+    float wl = __shfl_up_sync(0xffffffffu, wix.v[3], 1);
+    float gl = __shfl_up_sync(0xffffffffu, gx.v[3], 1);
+    if (lane == 0 && j0 > 0) {
+        const float rxl = fsub(fsub(c.v[0], fsub(ul, m)), gxl);
+        wl = irls_w(wxl, rxl, eps2);
+        gl = gxl;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int j = j0 + q;
+        float b = 0.f;
+        if (j > 0) {
+            const float wleft = q == 0 ? wl : wix.v[q - 1];
+            const float gleft = q == 0 ? gl : gx.v[q - 1];
+            b = fadd(b, fmul(wleft, gleft));
         }
+        if (j < W - 1) b = fsub(b, fmul(wix.v[q], gx.v[q]));
+        if (hu) {
+            const float ryu = fsub(fsub(c.v[q], fsub(uu.v[q], m)), gyu.v[q]);
+            b = fadd(b, fmul(irls_w(wyu.v[q], ryu, eps2), gyu.v[q]));
+        }
+        if (hd) b = fsub(b, fmul(wiy.v[q], gy.v[q]));
+        bv.v[q] = b;
+        if (on && j < W) {
+            acc[0] += (double)fmul(rx.v[q], rx.v[q]) + (double)fmul(ry.v[q], ry.v[q]);
+            acc[1] += isfinite(c.v[q]) ? 0.0 : 1.0;
+        }
+    }
+    if (on) {
+        st4(un, o, c);
+        st4(G.wIx, o, wix);
+        st4(G.wIy, o, wiy);
+        st4(G.b, o, bv);
     }
     if (arrive<2>(G, local, nct, acc, red)) {
         finish_sum<2>(G, nct, acc, red);
@@ -526,6 +565,12 @@ __global__ void __launch_bounds__(256) k_head(const GridDev* __restrict__ grids,
 }
 
 // ============================================================ elementwise kernels (KS_ELEM)
+// A CTA takes whole rows (grid-stride over rows), threads take float4 column
+// groups; P is a multiple of 4, so a group starting below W stays in the row.
+#define UNW_ROWS_LOOP(G, local, nct)                          \
+    for (int i = (local); i < (G).H; i += (nct))              \
+        for (int j = 4 * threadIdx.x; j < (G).W; j += 4 * blockDim.x)
+
 // sum over all pixels of u * valid (utils_unwrap2d.py:1539-1541)
 __global__ void k_mean(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n, int it) {
     __shared__ double red[32 * 1];
@@ -535,14 +580,16 @@ __global__ void k_mean(const GridDev* __restrict__ grids, const int* __restrict_
     if (!st->irls_active) return;
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
-    const int W = G.W, P = G.P;
-    const long long npx = (long long)G.H * W;
     const float* __restrict__ uc = (it & 1) ? G.U1 : G.U0;
     double acc[1] = {0.0};
-    for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
-        const int i = (int)(q / W), j = (int)(q - (long long)i * W);
-        const size_t o = (size_t)i * P + j;
-        acc[0] += (double)(uc[o] * (G.valid[o] ? 1.f : 0.f));
+    UNW_ROWS_LOOP(G, local, nct) {
+        const size_t o = (size_t)i * G.P + j;
+        const F4 u = ld4(uc, o);
+        const uchar4 v = *reinterpret_cast<const uchar4*>(G.valid + o);
+        const unsigned char vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (j + q < G.W) acc[0] += (double)(u.v[q] * (vv[q] ? 1.f : 0.f));
     }
     if (arrive<1>(G, local, nct, acc, red)) {
         finish_sum<1>(G, nct, acc, red);
@@ -557,15 +604,14 @@ __global__ void k_init_recentre(const GridDev* __restrict__ grids, const int* __
     const InstState* st = G.st;
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
-    const int W = G.W, P = G.P;
-    const long long npx = (long long)G.H * W;
     const float m = st->vcount > 0 ? (float)st->mean : 0.f;
-    for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
-        const int i = (int)(q / W), j = (int)(q - (long long)i * W);
-        const size_t o = (size_t)i * P + j;
-        const float u = fsub(G.U0[o], m);
-        G.U0[o] = u;
-        G.Ub[o] = u;
+    UNW_ROWS_LOOP(G, local, nct) {
+        const size_t o = (size_t)i * G.P + j;
+        F4 u = ld4(G.U0, o);
+#pragma unroll
+        for (int q = 0; q < 4; q++) u.v[q] = fsub(u.v[q], m);
+        st4(G.U0, o, u);
+        st4(G.Ub, o, u);
     }
 }
 
@@ -577,13 +623,10 @@ __global__ void k_copy_best(const GridDev* __restrict__ grids, const int* __rest
     if (!(st->irls_active && st->best_update)) return;
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
-    const int W = G.W, P = G.P;
-    const long long npx = (long long)G.H * W;
     const float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
-    for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
-        const int i = (int)(q / W), j = (int)(q - (long long)i * W);
-        const size_t o = (size_t)i * P + j;
-        G.Ub[o] = un[o];
+    UNW_ROWS_LOOP(G, local, nct) {
+        const size_t o = (size_t)i * G.P + j;
+        st4(G.Ub, o, ld4(un, o));
     }
 }
 
@@ -597,19 +640,20 @@ __global__ void k_rel(const GridDev* __restrict__ grids, const int* __restrict__
     if (!st->irls_active) return;
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
-    const int W = G.W, P = G.P;
-    const long long npx = (long long)G.H * W;
     const float* __restrict__ up = (it & 1) ? G.U1 : G.U0;
     const float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
     double acc[3] = {0.0, 0.0, 0.0};
-    for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
-        const int i = (int)(q / W), j = (int)(q - (long long)i * W);
-        const size_t o = (size_t)i * P + j;
-        const float u = un[o];
-        const float d = fsub(up[o], u);
-        acc[0] += (double)d * (double)d;
-        acc[1] += (double)u * (double)u;
-        acc[2] += isfinite(u) ? 0.0 : 1.0;
+    UNW_ROWS_LOOP(G, local, nct) {
+        const size_t o = (size_t)i * G.P + j;
+        const F4 u = ld4(un, o), v = ld4(up, o);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (j + q >= G.W) break;
+            const float d = fsub(v.v[q], u.v[q]);
+            acc[0] += (double)d * (double)d;
+            acc[1] += (double)u.v[q] * (double)u.v[q];
+            acc[2] += isfinite(u.v[q]) ? 0.0 : 1.0;
+        }
     }
     if (arrive<3>(G, local, nct, acc, red)) {
         finish_sum<3>(G, nct, acc, red);
