@@ -6,5 +6,6 @@ libunwrap_b200.so (hand-written CUDA kernels behind the C ABI in
 include/unwrap_b200.h); PyTorch supplies device memory and the stream.
 """
 from .unwrap2d import irls_unwrap_2d, irls_unwrap_2d_batch, resolve_device  # noqa: F401
+from .adapters import unwrap2d_chunk  # noqa: F401
 
-__all__ = ["irls_unwrap_2d", "irls_unwrap_2d_batch"]
+__all__ = ["irls_unwrap_2d", "irls_unwrap_2d_batch", "unwrap2d_chunk"]
