@@ -43,10 +43,10 @@ UNIT = "Mpx/s"
 # Algorithmic HBM bytes per pixel per launch of each kernel family (float32 words,
 # halo re-reads and reduction partials not counted).
 ALG_BYTES = {
-    "matvec": 24.0,    # read z, p_old, wIx, wIy; write p, Ap
+    "matvec": 16.0,    # read p, wIx, wIy; write Ap
     "row_upd": 28.0,   # read x, p, r, Ap; write x, r, T
     "col": 8.0,        # read T; write T
-    "row_inv": 12.0,   # read T, r; write z
+    "row_inv": 12.0,   # read T, p; write p (p = z + beta p in place)
     "head": 40.0,      # read u, gx, gy, wx, wy; write u, wIx, wIy, b (+ halo)
     "row_r0": 24.0,    # read b, x, wIx, wIy; write r, T
 }
@@ -295,6 +295,7 @@ def run_b200(args):
                           "us_per_launch": round(float(kms) / kn * 1e3, 2),
                           "gbs": round(ALG_BYTES[k] * npx / (kms / 1e3 / kn) / 1e9, 1)}
     pcg_ms = sum(fam[k][0] for k in ("matvec", "row_upd", "col", "row_inv"))
+    pcg_bpx = sum(ALG_BYTES[k] for k in ("matvec", "row_upd", "col", "row_inv"))
     n_pcg = max(int(fam["matvec"][1]), 1)
     traffic = None
     tf = os.path.join(REPO, "profiles", "traffic.json")
@@ -304,8 +305,8 @@ def run_b200(args):
                 "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": dom,
                 "peak_source": peak_kind,
                 "alg_bytes_per_launch": ALG_BYTES[dom] * npx,
-                "pcg_iteration": {"us": round(pcg_ms / n_pcg * 1e3, 1), "alg_bytes_per_px": 72.0,
-                                  "gbs": round(72.0 * npx / (pcg_ms / 1e3 / n_pcg) / 1e9, 1)},
+                "pcg_iteration": {"us": round(pcg_ms / n_pcg * 1e3, 1), "alg_bytes_per_px": pcg_bpx,
+                                  "gbs": round(pcg_bpx * npx / (pcg_ms / 1e3 / n_pcg) / 1e9, 1)},
                 "kernels": kernels}
 
     # ---- CPU baseline (rank 0, N=1 only): the oracle on a bounded sample

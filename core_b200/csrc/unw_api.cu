@@ -310,7 +310,7 @@ int enqueue_iteration(Solver& S, int t) {
     for (int k = 0; k < S.sc.cg_max_iter; k++) {
         PL(UNW_PROF_MATVEC, unw_launch_simple(UNW_K_MATVEC, S.total[KS_MATVEC], s, S.dg, S.ds(KS_MATVEC), n, k, S.sc));
         PL(UNW_PROF_ROW_UPD, L_rowf(S, 2, t, k));
-        PL(UNW_PROF_COL, L_col(S, 1));
+        PL(UNW_PROF_COL, L_col(S, 2));
         PL(UNW_PROF_ROW_INV, L_rowi(S, 2));
     }
     PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_REL, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));

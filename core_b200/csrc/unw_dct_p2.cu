@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowf_p2(const 
     const int H = G.H, P = G.P;
     const int t = threadIdx.x;
     float* U = (it & 1) ? G.U0 : G.U1;
-    const float* pk = (MODE == 2) ? ((cgk & 1) ? G.p1 : G.p0) : nullptr;
+    const float* pk = (MODE == 2) ? G.p0 : nullptr;
     const float alpha = (MODE == 2) ? st->alpha : 0.f;
     double acc[2] = {0.0, 0.0};
     for (int pair = local; pair < (H + 1) / 2; pair += nct) {
@@ -148,7 +148,8 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowf_p2(const 
 
 // Epilogue of the row-inverse pass for columns j..j+3 of row i.
 template <int MODE>
-__device__ __forceinline__ void rowi_store4(const GridDev& G, int i, int j, float4 z, double (&acc)[2]) {
+__device__ __forceinline__ void rowi_store4(const GridDev& G, int i, int j, float4 z, float beta,
+                                            double (&acc)[2]) {
     const size_t o = (size_t)i * G.P + j;
     if (MODE == 3) {
         st4f(G.z, o, z);
@@ -161,10 +162,12 @@ __device__ __forceinline__ void rowi_store4(const GridDev& G, int i, int j, floa
         const uchar4 v = *reinterpret_cast<const uchar4*>(G.valid + o);
         acc[0] += (double)(u.x * (v.x ? 1.f : 0.f)) + (double)(u.y * (v.y ? 1.f : 0.f)) +
                   (double)(u.z * (v.z ? 1.f : 0.f)) + (double)(u.w * (v.w ? 1.f : 0.f));
+    } else if (MODE == 1) {
+        st4f(G.p0, o, z);
     } else {
-        st4f(G.z, o, z);
-        const float4 r = ld4f(G.r, o);
-        acc[0] += (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z + (double)r.w * z.w;
+        const float4 p = ld4f(G.p0, o);
+        st4f(G.p0, o, make_float4(fadd(fmul(p.x, beta), z.x), fadd(fmul(p.y, beta), z.y),
+                                  fadd(fmul(p.z, beta), z.z), fadd(fmul(p.w, beta), z.w)));
     }
 }
 
@@ -183,15 +186,16 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
     const int H = G.H, P = G.P;
     const int t = threadIdx.x;
     const float2* __restrict__ dw = G.prow.dctw;
+    const float beta = MODE == 2 ? st->beta : 0.f;
     double acc[2] = {0.0, 0.0};
     for (int pair = local; pair < (H + 1) / 2; pair += nct) {
     const int i0 = 2 * pair, i1 = i0 + 1;
     const bool has1 = i1 < H;
     const float* __restrict__ Ta = G.T + (size_t)i0 * P;
     const float* __restrict__ Tb = G.T + (size_t)i1 * P;
-    if (MODE == 1 || MODE == 2) {
-        // the epilogue reads r of these rows after the FFT: start them towards L2 now
-        const float* ra = G.r + (size_t)i0 * P;
+    if (MODE == 2) {
+        // the epilogue reads p of these rows after the FFT: start them towards L2 now
+        const float* ra = G.p0 + (size_t)i0 * P;
         for (int c = t * 32; c < N; c += T * 32) {
             asm volatile("prefetch.global.L2 [%0];" ::"l"(ra + c));
             if (has1) asm volatile("prefetch.global.L2 [%0];" ::"l"(ra + P + c));
@@ -231,27 +235,29 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
             za[c] = v.x;
             zb[c] = -v.y;
         }
-        rowi_store4<MODE>(G, i0, j, make_float4(za[0], za[1], za[2], za[3]), acc);
-        if (has1) rowi_store4<MODE>(G, i1, j, make_float4(zb[0], zb[1], zb[2], zb[3]), acc);
+        rowi_store4<MODE>(G, i0, j, make_float4(za[0], za[1], za[2], za[3]), beta, acc);
+        if (has1) rowi_store4<MODE>(G, i1, j, make_float4(zb[0], zb[1], zb[2], zb[3]), beta, acc);
     }
     }
-    if (MODE == 3) return;
+    if (MODE != 0) return;
     if (arrive<2>(G, local, nct, acc, red)) {
         finish_sum<2>(G, nct, acc, red);
-        if (threadIdx.x == 0) rowinv_finalize<MODE>(st, acc);
+        if (threadIdx.x == 0) rowinv_finalize_initu(st, acc);
     }
 }
 
-// MODE 0: DCT initial solve (always runs); MODE 1: PCG (gated).
+// MODE 0: DCT initial solve (always runs); MODE 1 / 2: PCG (gated), also
+// r.z by Parseval and its scalar step (col_finalize).
 template <int N, int NSEQ, int MODE>
 __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_col_p2(
     const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
     constexpr int T = N / 16;
     extern __shared__ float2 sm[];
+    __shared__ double red[32];
     const int g = find_grid(starts, n, blockIdx.x);
     const GridDev& G = grids[g];
-    const InstState* st = G.st;
-    if (MODE == 1 && !(st->irls_active && st->cg_active)) return;
+    InstState* st = G.st;
+    if (MODE >= 1 && !(st->irls_active && st->cg_active)) return;
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const int W = G.W, P = G.P;
@@ -263,6 +269,7 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
     const float* __restrict__ sH = G.sH;
     const float negs = -1.0f / (4.0f * (float)N * (float)W);
     const int nslab = (W + 2 * NSEQ - 1) / (2 * NSEQ);
+    double acc[1] = {0.0};
     for (int slab = local; slab < nslab; slab += nct) {
     const int ja = 2 * NSEQ * slab + 2 * s;
     const bool hasa = ja < W, hasb = ja + 1 < W;
@@ -291,7 +298,7 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
         const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
         const float ck = __ldg(&sH[k]), cm = __ldg(&sH[km]);
         float2 ok, om;
-        col_spectral_pair(C, Cm, k, km, wk, wm, ck, cm, ca, cb, ja == 0, hasb, negs, ok, om);
+        col_spectral_pair<(MODE >= 1)>(C, Cm, k, km, wk, wm, ck, cm, ca, cb, ja == 0, hasb, negs, ok, om, acc[0]);
         if (km != k) sms[pad16(km)] = om;
         sms[pad16(k)] = ok;
     }
@@ -304,6 +311,11 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
         else if (hasb) { a[0] = v[q].x; a[1] = -v[q].y; }
         else if (hasa) a[0] = v[q].x;
     }
+    }
+    if (MODE == 0) return;
+    if (arrive<1>(G, local, nct, acc, red)) {
+        finish_sum<1>(G, nct, acc, red);
+        if (threadIdx.x == 0) col_finalize<MODE>(st, acc[0]);
     }
 }
 
@@ -354,7 +366,11 @@ static cudaError_t col_p2_n(int mode, int nblk, cudaStream_t s, const GridDev* g
         kfn<<<nblk, N / 16 * NS, smem, s>>>(gd, st, n);
         return cudaGetLastError();
     };
-    return mode == 0 ? go(k_col_p2<N, NS, 0>) : go(k_col_p2<N, NS, 1>);
+    switch (mode) {
+        case 0: return go(k_col_p2<N, NS, 0>);
+        case 1: return go(k_col_p2<N, NS, 1>);
+        default: return go(k_col_p2<N, NS, 2>);
+    }
 }
 
 int unw_p2_col_nseq(int N) {

@@ -46,7 +46,6 @@ struct InstState {
     float alpha, beta;
     int cg_active;
     int cg_iter;
-    int pfirst;
     // IRLS (utils_unwrap2d.py:1529-1632)
     int irls_active;
     int irls_iter;

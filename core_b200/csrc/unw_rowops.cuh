@@ -76,9 +76,11 @@ __device__ __forceinline__ void rowfwd_finalize(InstState* st, const double (&ac
 
 // Row-inverse modes:
 //  0 INITU u = nan_to_num(z) (utils_unwrap2d.py:1498-1502), sum of u * valid
-//  1 Z0    z = M^-1 r, rz = r.z                (utils_unwrap2d.py:1421-1428)
-//  2 Z     z = M^-1 r, beta from r.z          (utils_unwrap2d.py:1461-1472)
+//  1 P0    p = z = M^-1 r                     (utils_unwrap2d.py:1421-1424)
+//  2 P     p = z + beta p, z = M^-1 r         (utils_unwrap2d.py:1461-1473)
 //  3 COPY  z as computed (operator entry point)
+// r.z and beta come from the column pass (Parseval, col_finalize), so modes 1
+// and 2 write p in place and never store z.
 template <int MODE>
 __device__ __forceinline__ bool rowinv_gate(const InstState* s) {
     if (MODE == 0 || MODE == 3) return true;
@@ -86,7 +88,8 @@ __device__ __forceinline__ bool rowinv_gate(const InstState* s) {
 }
 
 template <int MODE>
-__device__ __forceinline__ void rowinv_store(const GridDev& G, int i, int j, float zv, double (&acc)[2]) {
+__device__ __forceinline__ void rowinv_store(const GridDev& G, int i, int j, float zv, float beta,
+                                             double (&acc)[2]) {
     const size_t o = (size_t)i * G.P + j;
     if (MODE == 3) {
         G.z[o] = zv;
@@ -96,21 +99,27 @@ __device__ __forceinline__ void rowinv_store(const GridDev& G, int i, int j, flo
         G.U0[o] = u;
         // (u * valid_float).sum(): an invalid pixel contributes u * 0
         acc[0] += (double)(u * (G.valid[o] ? 1.f : 0.f));
+    } else if (MODE == 1) {
+        G.p0[o] = zv;
     } else {
-        G.z[o] = zv;
-        acc[0] += (double)G.r[o] * (double)zv;
+        // _cg_p.mul_(beta).add_(_cg_z): one rounding per operation
+        G.p0[o] = fadd(fmul(G.p0[o], beta), zv);
     }
 }
 
+__device__ __forceinline__ void rowinv_finalize_initu(InstState* st, const double (&acc)[2]) {
+    if (acc[1] != 0.0) st->status |= 1;  // UNW_S_DCT_INIT_NONFINITE
+    st->mean = st->vcount > 0 ? acc[0] / st->vcount : 0.0;
+}
+
+// Last CTA of a PCG column pass: r.z of the new preconditioned residual.
+// MODE 1 starts the recurrence (utils_unwrap2d.py:1427); MODE 2 applies the
+// reference's test on the previous r.z, then beta (utils_unwrap2d.py:1464-1473).
 template <int MODE>
-__device__ __forceinline__ void rowinv_finalize(InstState* st, const double (&acc)[2]) {
-    if (MODE == 0) {
-        if (acc[1] != 0.0) st->status |= 1;  // UNW_S_DCT_INIT_NONFINITE
-        st->mean = st->vcount > 0 ? acc[0] / st->vcount : 0.0;
-    } else if (MODE == 1) {
-        st->rz = acc[0];
+__device__ __forceinline__ void col_finalize(InstState* st, double rzn) {
+    if (MODE == 1) {
+        st->rz = rzn;
     } else if (MODE == 2) {
-        const double rzn = acc[0];
         if (fabs(st->rz) < 1e-15) {
             st->cg_active = 0;
         } else {
@@ -126,19 +135,33 @@ __device__ __forceinline__ void rowinv_finalize(InstState* st, const double (&ac
 // (k, km = H-k): the DCT-II extraction and the eigenvalue scaling are shared,
 // only the DCT-III pre-twiddles differ.  For k = 0 (km = 0) or k = km the
 // second output equals the first and is not used.
+//
+// RZ adds this pair's share of r.z to `rz` by Parseval's identity for the
+// unnormalised DCT-II / DCT-III pair: with X the 2-D DCT-II of r and Y the
+// scaled spectrum that the DCT-III turns into z,
+//     r.z = sum_{k,l} e_k e_l X_kl Y_kl,   e_0 = 1/2, e_{k>0} = 1,
+// so the preconditioned inner product needs no extra pass over r and z.
+template <bool RZ>
 __device__ __forceinline__ void col_spectral_pair(float2 C, float2 Cm, int k, int km, float2 wk, float2 wm,
                                                   float ck, float cm, float ca, float cb, bool ja0, bool hasb,
-                                                  float negs, float2& ok, float2& om) {
+                                                  float negs, float2& ok, float2& om, double& rz) {
     const float2 Vak = make_float2(C.x + Cm.x, C.y - Cm.y);
     const float2 Vbk = make_float2(C.y + Cm.y, Cm.x - C.x);
     const float2 Vam = make_float2(Vak.x, -Vak.y);   // conj: the pair's extraction is symmetric
     const float2 Vbm = make_float2(Vbk.x, -Vbk.y);
-    float Xak = wk.x * Vak.x - wk.y * Vak.y, Xbk = wk.x * Vbk.x - wk.y * Vbk.y;
-    float Xam = wm.x * Vam.x - wm.y * Vam.y, Xbm = wm.x * Vbm.x - wm.y * Vbm.y;
-    Xak = (k == 0 && ja0) ? 0.f : Xak * __frcp_rn(-(ck + ca)) * negs;
-    Xam = (km == 0 && ja0) ? 0.f : Xam * __frcp_rn(-(cm + ca)) * negs;
-    Xbk = hasb ? Xbk * __frcp_rn(-(ck + cb)) * negs : 0.f;
-    Xbm = hasb ? Xbm * __frcp_rn(-(cm + cb)) * negs : 0.f;
+    const float xak = wk.x * Vak.x - wk.y * Vak.y, xbk = wk.x * Vbk.x - wk.y * Vbk.y;
+    const float xam = wm.x * Vam.x - wm.y * Vam.y, xbm = wm.x * Vbm.x - wm.y * Vbm.y;
+    const float Xak = (k == 0 && ja0) ? 0.f : xak * __frcp_rn(-(ck + ca)) * negs;
+    const float Xam = (km == 0 && ja0) ? 0.f : xam * __frcp_rn(-(cm + ca)) * negs;
+    const float Xbk = hasb ? xbk * __frcp_rn(-(ck + cb)) * negs : 0.f;
+    const float Xbm = hasb ? xbm * __frcp_rn(-(cm + cb)) * negs : 0.f;
+    if (RZ) {
+        const float ea = ja0 ? 0.5f : 1.0f;
+        float tk = fmaf(xak * ea, Xak, xbk * Xbk);
+        if (k == 0) tk *= 0.5f;
+        const float tm = km != k ? fmaf(xam * ea, Xam, xbm * Xbm) : 0.f;
+        rz += (double)tk + (double)tm;
+    }
     // DCT-III pre-twiddle V'_k = conj(w_k) (Y_k - i Y_{H-k}) with Y_H = 0
     const float mak = k == 0 ? 0.f : Xam, mbk = k == 0 ? 0.f : Xbm;
     const float2 Pak = cmul(cconj(wk), make_float2(Xak, -mak));
@@ -147,30 +170,4 @@ __device__ __forceinline__ void col_spectral_pair(float2 C, float2 Cm, int k, in
     const float2 Pam = cmul(cconj(wm), make_float2(Xam, -Xak));
     const float2 Pbm = cmul(cconj(wm), make_float2(Xbm, -Xbk));
     om = cconj(make_float2(Pam.x - Pbm.y, Pam.y + Pbm.x));
-}
-
-// Column-pass spectral step for one frequency pair (k, H-k) of two columns
-// (ja, ja+1) whose DFT outputs are C = C_k and Cm = C_{H-k}: DCT-II extraction,
-// division by the Neumann-Laplacian eigenvalue lambda = -(sH + sW) (see
-// GridDev::sH), negation, DC term zeroed, then the DCT-III pre-twiddle.
-// Returns conj(C'_k) ready for a forward FFT.  negs = -1/(4 H W) folds the
-// transform normalisations; with lambda = -(s) the factor is +1/(4 H W s).
-__device__ __forceinline__ float2 col_spectral(float2 C, float2 Cm, int k, int km, float2 wk, float2 wm,
-                                               float ck, float cm, float ca, float cb, bool ja0, bool hasb,
-                                               float negs) {
-    const float2 Vak = make_float2(C.x + Cm.x, C.y - Cm.y);
-    const float2 Vbk = make_float2(C.y + Cm.y, Cm.x - C.x);
-    const float2 Vam = make_float2(Cm.x + C.x, Cm.y - C.y);
-    const float2 Vbm = make_float2(Cm.y + C.y, C.x - Cm.x);
-    float Xak = wk.x * Vak.x - wk.y * Vak.y, Xbk = wk.x * Vbk.x - wk.y * Vbk.y;
-    float Xam = wm.x * Vam.x - wm.y * Vam.y, Xbm = wm.x * Vbm.x - wm.y * Vbm.y;
-    // X / lambda as X * (1/lambda) with a correctly rounded reciprocal (lambda = -(ck + ca))
-    Xak = (k == 0 && ja0) ? 0.f : Xak * __frcp_rn(-(ck + ca)) * negs;
-    Xam = (km == 0 && ja0) ? 0.f : Xam * __frcp_rn(-(cm + ca)) * negs;
-    Xbk = hasb ? Xbk * __frcp_rn(-(ck + cb)) * negs : 0.f;
-    Xbm = hasb ? Xbm * __frcp_rn(-(cm + cb)) * negs : 0.f;
-    const float mak = k == 0 ? 0.f : Xam, mbk = k == 0 ? 0.f : Xbm;
-    const float2 Pak = cmul(cconj(wk), make_float2(Xak, -mak));
-    const float2 Pbk = cmul(cconj(wk), make_float2(Xbk, -mbk));
-    return cconj(make_float2(Pak.x - Pbk.y, Pak.y + Pbk.x));
 }

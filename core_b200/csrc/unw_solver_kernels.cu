@@ -74,7 +74,7 @@ __global__ void k_state_init(const GridDev* __restrict__ grids, int n, UnwScalar
     if (g >= n) return;
     InstState* s = grids[g].st;
     s->rz = 0; s->pAp = 0; s->rnorm = 0; s->alpha = 0.f; s->beta = 0.f;
-    s->cg_active = 0; s->cg_iter = 0; s->pfirst = 1;
+    s->cg_active = 0; s->cg_iter = 0;
     s->irls_active = sc.max_iter > 0; s->irls_iter = 0; s->max_iter = sc.max_iter;
     s->best_update = 0; s->revert = 0; s->u_index = 0; s->status = 0;
     s->vcount = 0; s->mean = 0; s->residual = 0; s->best_residual = INFINITY; s->rel_change = 0;
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(T) k_row_fwd(const GridDev* __restrict__ grids
     const int H = G.H, W = G.W, P = G.P;
     double acc[2] = {0.0, 0.0};
     float* U = (it & 1) ? G.U0 : G.U1;  // x of this IRLS iteration (U_nxt)
-    const float* pk = (MODE == 2) ? ((cgk & 1) ? G.p1 : G.p0) : nullptr;
+    const float* pk = (MODE == 2) ? G.p0 : nullptr;
     const float alpha = (MODE == 2) ? st->alpha : 0.f;
     for (int pair = local; pair < (H + 1) / 2; pair += nct) {
     const int i0 = 2 * pair, i1 = i0 + 1;
@@ -192,19 +192,22 @@ __global__ void __launch_bounds__(T) k_row_fwd(const GridDev* __restrict__ grids
 
 // ============================================================ column pass
 // Column DCT-II -> scale by -1/(4 H W lambda) -> column DCT-III, in place on T.
-// MODE 0: DCT initial solve (always runs); MODE 1: PCG (gated).
+// MODE 0: DCT initial solve (always runs); MODE 1 / 2: PCG (gated), also
+// r.z by Parseval and its scalar step (col_finalize).
 template <int T, int EMAX, int MODE>
 __global__ void __launch_bounds__(T) k_col(const GridDev* __restrict__ grids,
                                            const int* __restrict__ starts, int n) {
     extern __shared__ float2 sm[];
+    __shared__ double red[32];
     const int g = find_grid(starts, n, blockIdx.x);
     const GridDev& G = grids[g];
-    const InstState* st = G.st;
-    if (MODE == 1 && !(st->irls_active && st->cg_active)) return;
+    InstState* st = G.st;
+    if (MODE >= 1 && !(st->irls_active && st->cg_active)) return;
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
     const int nslab = (W + 2 * G.col_nseq - 1) / (2 * G.col_nseq);
+    double acc[1] = {0.0};
     for (int slab = local; slab < nslab; slab += nct) {
     const int c0 = 2 * G.col_nseq * slab;
     const int nseq = min(G.col_nseq, (W - c0 + 1) >> 1);
@@ -236,8 +239,10 @@ __global__ void __launch_bounds__(T) k_col(const GridDev* __restrict__ grids,
         const bool hasb = ja + 1 < W;
         const float ca = sW[ja], cb = hasb ? sW[ja + 1] : 1.0f;
         const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
-        const float2 ok = col_spectral(C, Cm, k, km, wk, wm, sH[k], sH[km], ca, cb, ja == 0, hasb, negs);
-        if (km != k) base[km] = col_spectral(Cm, C, km, k, wm, wk, sH[km], sH[k], ca, cb, ja == 0, hasb, negs);
+        float2 ok, om;
+        col_spectral_pair<(MODE >= 1)>(C, Cm, k, km, wk, wm, sH[k], sH[km], ca, cb, ja == 0, hasb, negs, ok, om,
+                                     acc[0]);
+        if (km != k) base[km] = om;
         base[k] = ok;
     }
     __syncthreads();
@@ -249,6 +254,11 @@ __global__ void __launch_bounds__(T) k_col(const GridDev* __restrict__ grids,
         Tm[(size_t)i * P + c] = v.x;
         if (c + 1 < W) Tm[(size_t)i * P + c + 1] = -v.y;
     }
+    }
+    if (MODE == 0) return;
+    if (arrive<1>(G, local, nct, acc, red)) {
+        finish_sum<1>(G, nct, acc, red);
+        if (threadIdx.x == 0) col_finalize<MODE>(st, acc[0]);
     }
 }
 
@@ -267,6 +277,7 @@ __global__ void __launch_bounds__(T) k_row_inv(const GridDev* __restrict__ grids
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
+    const float beta = MODE == 2 ? st->beta : 0.f;
     double acc[2] = {0.0, 0.0};
     for (int pair = local; pair < (H + 1) / 2; pair += nct) {
     const int i0 = 2 * pair, i1 = i0 + 1;
@@ -300,14 +311,14 @@ __global__ void __launch_bounds__(T) k_row_inv(const GridDev* __restrict__ grids
     dft_n<T, EMAX>(sm, 1, G.prow);
     for (int j = threadIdx.x; j < W; j += T) {
         const float2 v = sm[mk_perm(j, W)];
-        rowinv_store<MODE>(G, i0, j, v.x, acc);
-        if (has1) rowinv_store<MODE>(G, i1, j, -v.y, acc);
+        rowinv_store<MODE>(G, i0, j, v.x, beta, acc);
+        if (has1) rowinv_store<MODE>(G, i1, j, -v.y, beta, acc);
     }
     }
-    if (MODE == 3) return;
+    if (MODE != 0) return;
     if (arrive<2>(G, local, nct, acc, red)) {
         finish_sum<2>(G, nct, acc, red);
-        if (threadIdx.x == 0) rowinv_finalize<MODE>(st, acc);
+        if (threadIdx.x == 0) rowinv_finalize_initu(st, acc);
     }
 }
 
@@ -342,11 +353,12 @@ __device__ __forceinline__ float pnew1(const float* __restrict__ z, const float*
     return first ? z[o] : fadd(fmul(po[o], beta), z[o]);
 }
 
-// matvec: p = z + beta p_old, Ap = A p, pAp = p.Ap (utils_unwrap2d.py:1430-1443, :1471).
+// matvec: Ap = A p, pAp = p.Ap (utils_unwrap2d.py:1430-1436).  p is formed in
+// place by the row-inverse pass, so this kernel only reads it.
 // A CTA is 16 warps over a 128-column x 16-row tile; each warp computes one row
-// (4 columns per lane) and issues all its loads (rows i-1, i, i+1 of z and
-// p_old, the weights, the tile-edge scalars) before using any of them.  The
-// neighbouring rows come back from L1/L2: DRAM traffic stays one pass per array.
+// (4 columns per lane) and issues all its loads (rows i-1, i, i+1 of p, the
+// weights, the tile-edge scalars) before using any of them.  The neighbouring
+// rows come back from L1/L2: DRAM traffic stays one pass per array.
 __global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ grids,
                                                    const int* __restrict__ starts, int n, int k) {
     __shared__ double red[32 * 1];
@@ -358,11 +370,7 @@ __global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ g
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool first = st->pfirst != 0;
-    const float beta = st->beta;
-    const float* __restrict__ z = G.z;
-    const float* __restrict__ po = (k & 1) ? G.p0 : G.p1;
-    float* __restrict__ pn = (k & 1) ? G.p1 : G.p0;
+    const float* __restrict__ p = G.p0;
     double acc[1] = {0.0};
     const int ntiles = G.sten_tiles_x * ((H + 15) / 16);
     for (int tile = local; tile < ntiles; tile += nct) {
@@ -373,40 +381,20 @@ __global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ g
     const bool on = i < H && j0 < W;
     const bool hu = i > 0, hd = i < H - 1;
     const size_t o = (size_t)i * P + j0;
-    F4 zc{}, zu{}, zd{}, qc{}, qu{}, qd{}, wx{}, wy{}, wyu{};
-    float zl = 0.f, ql = 0.f, wl = 0.f, zr = 0.f, qr = 0.f;
+    F4 cur{}, up{}, dn{}, wx{}, wy{}, wyu{};
+    float zl = 0.f, wl = 0.f, zr = 0.f;
     if (on) {
-        zc = ld4(z, o);
-        if (hu) zu = ld4(z, o - P);
-        if (hd) zd = ld4(z, o + P);
-        if (!first) {
-            qc = ld4(po, o);
-            if (hu) qu = ld4(po, o - P);
-            if (hd) qd = ld4(po, o + P);
-        }
+        cur = ld4(p, o);
+        if (hu) up = ld4(p, o - P);
+        if (hd) dn = ld4(p, o + P);
         wx = ld4(G.wIx, o);
         wy = ld4(G.wIy, o);
         if (hu) wyu = ld4(G.wIy, o - P);
         if (lane == 0 && j0 > 0) {
-            zl = z[o - 1];
-            if (!first) ql = po[o - 1];
+            zl = p[o - 1];
             wl = G.wIx[o - 1];
         }
-        if (lane == 31 && j0 + 4 < W) {
-            zr = z[o + 4];
-            if (!first) qr = po[o + 4];
-        }
-    }
-    F4 cur = zc, up = zu, dn = zd;
-    if (!first) {
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            cur.v[c] = fadd(fmul(qc.v[c], beta), zc.v[c]);
-            up.v[c] = fadd(fmul(qu.v[c], beta), zu.v[c]);
-            dn.v[c] = fadd(fmul(qd.v[c], beta), zd.v[c]);
-        }
-        zl = fadd(fmul(ql, beta), zl);
-        zr = fadd(fmul(qr, beta), zr);
+        if (lane == 31 && j0 + 4 < W) zr = p[o + 4];
     }
     float pl = __shfl_up_sync(0xffffffffu, cur.v[3], 1);
     float wll = __shfl_up_sync(0xffffffffu, wx.v[3], 1);
@@ -430,7 +418,6 @@ __global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ g
             ap.v[c] = -res;
             if (j < W) acc[0] += (double)pc * (double)ap.v[c];
         }
-        st4(pn, o, cur);
         st4(G.Ap, o, ap);
     }
     }
@@ -440,7 +427,6 @@ __global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ g
             const double pAp = acc[0];
             st->pAp = pAp;
             st->cg_iter += 1;
-            st->pfirst = 0;
             if (fabs(pAp) < 1e-15 || !isfinite(pAp)) {
                 st->cg_active = 0;
             } else {
@@ -559,7 +545,6 @@ __global__ void __launch_bounds__(256) k_head(const GridDev* __restrict__ grids,
             }
             st->cg_active = 1;
             st->cg_iter = 0;
-            st->pfirst = 1;
         }
     }
 }
@@ -764,8 +749,11 @@ cudaError_t unw_launch_col(int mode, int T, int emax, int nblk, size_t smem, cud
                            const GridDev* gd, const int* starts, int n) {
     if (nblk <= 0) return cudaSuccess;
     dim3 grid(nblk);
-    return mode == 0 ? launch_col_t<0>(T, emax, grid, smem, s, gd, starts, n)
-                     : launch_col_t<1>(T, emax, grid, smem, s, gd, starts, n);
+    switch (mode) {
+        case 0: return launch_col_t<0>(T, emax, grid, smem, s, gd, starts, n);
+        case 1: return launch_col_t<1>(T, emax, grid, smem, s, gd, starts, n);
+        default: return launch_col_t<2>(T, emax, grid, smem, s, gd, starts, n);
+    }
 }
 
 cudaError_t unw_launch_tables(const FftPlanDev& f, const DctPlanDev& d, float* sv, int Ncos,
