@@ -23,6 +23,7 @@ UNW_E_OVERFLOW = -5
 UNW_F_CONGRUENT = 1
 UNW_F_NO_GRAPH = 2
 UNW_F_PROFILE = 4
+UNW_F_FIXED_ITERS = 8
 
 PROF_NAMES = ["bbox", "setup", "row_rho", "col", "row_inv", "matvec", "row_upd", "row_r0", "head", "elem", "post"]
 PROF_N = len(PROF_NAMES)

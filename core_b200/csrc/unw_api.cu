@@ -317,6 +317,56 @@ int enqueue_iteration(Solver& S, int t) {
     return UNW_OK;
 }
 
+// One IRLS iteration as a CUDA graph.  Kernels only use the parity of the
+// iteration index (which U buffer is current), so two executable graphs cover
+// a whole solve.  Capture runs on a private non-blocking stream of this thread
+// (the caller's stream may be the legacy default stream, which cannot be
+// captured); the graphs are then launched on the caller's stream.
+struct IterGraphs {
+    cudaGraphExec_t ex[2] = {nullptr, nullptr};
+    ~IterGraphs() {
+        for (auto e : ex)
+            if (e) cudaGraphExecDestroy(e);
+    }
+};
+
+cudaStream_t capture_stream() {
+    thread_local std::map<int, cudaStream_t> streams;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    auto it = streams.find(dev);
+    if (it != streams.end()) return it->second;
+    cudaStream_t cs = nullptr;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    streams[dev] = cs;
+    return cs;
+}
+
+// Returns UNW_OK with both graphs built, or an error code; a failed capture
+// leaves no graph and no stream in capture mode.
+int build_iteration_graphs(Solver& S, IterGraphs& G) {
+    cudaStream_t cs = capture_stream();
+    if (!cs) return set_err(UNW_E_CUDA, "no capture stream");
+    cudaStream_t user = S.s;
+    for (int par = 0; par < 2; par++) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed));
+        S.s = cs;
+        const int rc = enqueue_iteration(S, par);
+        S.s = user;
+        const cudaError_t e = cudaStreamEndCapture(cs, &g);
+        if (rc != UNW_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return rc != UNW_OK ? rc : set_err(UNW_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&G.ex[par], g, 0);
+        cudaGraphDestroy(g);
+        CK(ei);
+    }
+    return UNW_OK;
+}
+
 int read_states(Solver& S, std::vector<InstState>& out) {
     out.resize(S.n);
     for (int g = 0; g < S.n; g++)
@@ -366,8 +416,9 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
     S.hg.resize(n);
     S.sc.max_iter = prm->max_iter;
     S.sc.cg_max_iter = prm->cg_max_iter;
-    S.sc.tol = prm->tol;
-    S.sc.cg_tol = prm->cg_tol;
+    const bool fixed = (prm->flags & UNW_F_FIXED_ITERS) != 0;
+    S.sc.tol = fixed ? 0.f : prm->tol;        // rel_change < 0 never holds
+    S.sc.cg_tol = fixed ? 0.f : prm->cg_tol;  // ||r|| < 0 never holds
     S.sc.eps2 = (float)((double)prm->epsilon * (double)prm->epsilon);
     S.sc.conncomp_size = prm->conncomp_size;
     std::vector<HostPlan> prow(n), pcol(n);
@@ -531,9 +582,19 @@ int solve_group(const std::vector<int>& idx, const unw_grid* grids, const std::v
         // 5. IRLS loop (utils_unwrap2d.py:1533-1626)
         const int every = std::max(1, prm->check_every);
         std::vector<InstState> hs;
-        for (int t = 0; t < prm->max_iter; t++) {
-            rc = enqueue_iteration(S, t);
+        IterGraphs graphs;
+        const bool use_graph = !S.prof.on && !(prm->flags & UNW_F_NO_GRAPH) && prm->max_iter >= 2;
+        if (use_graph) {
+            rc = build_iteration_graphs(S, graphs);
             if (rc) return rc;
+        }
+        for (int t = 0; t < prm->max_iter; t++) {
+            if (use_graph) {
+                CK(cudaGraphLaunch(graphs.ex[t & 1], s));
+            } else {
+                rc = enqueue_iteration(S, t);
+                if (rc) return rc;
+            }
             if ((t + 1) % every == 0 || t + 1 == prm->max_iter) {
                 rc = read_states(S, hs);
                 if (rc) return rc;

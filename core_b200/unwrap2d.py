@@ -53,7 +53,7 @@ def resolve_device(device, phase=None):
 
 
 def make_params(max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2, conncomp_size=30,
-                congruent=False, check_every=1):
+                congruent=False, check_every=1, fixed_iters=False):
     p = _lib.UnwParams()
     p.max_iter = int(max_iter)
     p.tol = float(tol)
@@ -61,7 +61,7 @@ def make_params(max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2
     p.cg_tol = float(cg_tol)
     p.epsilon = float(epsilon)
     p.conncomp_size = int(conncomp_size)
-    p.flags = _lib.UNW_F_CONGRUENT if congruent else 0
+    p.flags = (_lib.UNW_F_CONGRUENT if congruent else 0) | (_lib.UNW_F_FIXED_ITERS if fixed_iters else 0)
     p.check_every = int(check_every)
     return p
 
@@ -104,7 +104,7 @@ def _ws():
 
 def irls_unwrap_2d(phase, weight=None, device='auto', max_iter=50, tol=1e-3,
                    cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2, conncomp_size=30, debug=False,
-                   *, congruent=False, return_stats=False, check_every=1):
+                   *, congruent=False, return_stats=False, check_every=1, fixed_iters=False):
     """Unwrap 2-D phase with the DCT-preconditioned IRLS L1 solver on a B200.
 
     Same parameters and outputs as the reference (utils_unwrap2d.py:1082-1083).
@@ -112,6 +112,8 @@ def irls_unwrap_2d(phase, weight=None, device='auto', max_iter=50, tol=1e-3,
       congruent     return phase + 2*pi*round((u - phase)/2pi) instead of u
       return_stats  also return a dict of iteration counts and status bits
       check_every   IRLS iterations enqueued between device->host convergence reads
+      fixed_iters   run exactly max_iter x cg_max_iter iterations (tol / cg_tol stop
+                    tests off, numerical breaks kept): identical work for timing
     """
     torch = _torch()
     is_torch = isinstance(phase, torch.Tensor)
@@ -130,7 +132,8 @@ def irls_unwrap_2d(phase, weight=None, device='auto', max_iter=50, tol=1e-3,
         nbytes = lib.unw_workspace_bytes(H, W)
         ws = _ws().get(dev, nbytes)
         st = _lib.UnwStats()
-        prm = make_params(max_iter, tol, cg_max_iter, cg_tol, epsilon, conncomp_size, congruent, check_every)
+        prm = make_params(max_iter, tol, cg_max_iter, cg_tol, epsilon, conncomp_size, congruent, check_every,
+                          fixed_iters)
         stream = torch.cuda.current_stream(dev).cuda_stream
         rc = lib.unw_solve_f32(ph.data_ptr(), W, wt.data_ptr() if wt is not None else None, W, H, W,
                                C.byref(prm), out_u.data_ptr(), W, out_cc.data_ptr(), W,
@@ -157,7 +160,7 @@ def irls_unwrap_2d(phase, weight=None, device='auto', max_iter=50, tol=1e-3,
 
 def irls_unwrap_2d_batch(phases, weights=None, device='auto', max_iter=50, tol=1e-3, cg_max_iter=20,
                          cg_tol=1e-4, epsilon=1e-2, conncomp_size=30, debug=False, *, congruent=False,
-                         return_stats=False, check_every=1):
+                         return_stats=False, check_every=1, fixed_iters=False):
     """Unwrap a list of independent grids (any sizes) in one batched launch sequence.
 
     Each grid converges on its own test, exactly as if `irls_unwrap_2d` had been
@@ -205,7 +208,8 @@ def irls_unwrap_2d_batch(phases, weights=None, device='auto', max_iter=50, tol=1
         nbytes = lib.unw_batch_workspace_bytes(n, Hs, Ws)
         ws = _ws().get(dev, nbytes)
         sts = (_lib.UnwStats * n)()
-        prm = make_params(max_iter, tol, cg_max_iter, cg_tol, epsilon, conncomp_size, congruent, check_every)
+        prm = make_params(max_iter, tol, cg_max_iter, cg_tol, epsilon, conncomp_size, congruent, check_every,
+                          fixed_iters)
         rc = lib.unw_solve_batch(n, grids, C.byref(prm), ws.data_ptr(), ws.numel(), sts,
                                  torch.cuda.current_stream(dev).cuda_stream)
         _lib.check(rc, "unw_solve_batch")

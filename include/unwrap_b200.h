@@ -57,6 +57,9 @@ typedef struct unw_params {
 #define UNW_F_CONGRUENT 1   /* output phase + 2*pi*k instead of the smooth solution */
 #define UNW_F_NO_GRAPH  2   /* launch kernels one by one instead of a CUDA graph    */
 #define UNW_F_PROFILE   4   /* time every kernel launch with CUDA events (unw_stats.prof_*) */
+#define UNW_F_FIXED_ITERS 8 /* run max_iter IRLS x cg_max_iter PCG iterations: the tol and
+                               cg_tol stop tests are off, the numerical breaks stay (for
+                               comparing throughput at identical work)                      */
 
 /* Kernel families timed under UNW_F_PROFILE (index into unw_stats.prof_*). */
 enum {

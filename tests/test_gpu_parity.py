@@ -324,3 +324,50 @@ def test_repeat_calls_on_reused_workspace_are_identical():
     u2, c2 = core_b200.irls_unwrap_2d(p, c)
     np.testing.assert_array_equal(u1, u2)
     np.testing.assert_array_equal(c1, c2)
+
+
+def _solve_flags(p, c, flags, **kw):
+    from core_b200.unwrap2d import make_params
+    lib = _lib.load()
+    H, W = p.shape
+    ph = torch.from_numpy(np.ascontiguousarray(p, np.float32)).to(DEV)
+    wt = torch.from_numpy(np.ascontiguousarray(c, np.float32)).to(DEV)
+    ou = torch.empty((H, W), dtype=torch.float32, device=DEV)
+    oc = torch.empty((H, W), dtype=torch.int16, device=DEV)
+    ws = _ws(H, W)
+    prm = make_params(**kw)
+    prm.flags |= flags
+    st = _lib.UnwStats()
+    _lib.check(lib.unw_solve_f32(ph.data_ptr(), W, wt.data_ptr(), W, H, W, C.byref(prm), ou.data_ptr(), W,
+                                 oc.data_ptr(), W, ws.data_ptr(), ws.numel(), C.byref(st), _stream()))
+    torch.cuda.synchronize()
+    return ou.cpu().numpy(), oc.cpu().numpy(), st.as_dict()
+
+
+@pytest.mark.parametrize("shape", [(256, 256), (200, 300)])
+def test_graph_launches_equal_direct_launches(shape):
+    # the IRLS iterations run as two captured CUDA graphs unless UNW_F_NO_GRAPH is set;
+    # every kernel is deterministic, so both must give identical bits
+    p, c, _ = gen_g2(*shape, seed=7)
+    u1, c1, s1 = _solve_flags(p, c, 0)
+    u2, c2, s2 = _solve_flags(p, c, _lib.UNW_F_NO_GRAPH)
+    u3, c3, s3 = _solve_flags(p, c, _lib.UNW_F_PROFILE)
+    np.testing.assert_array_equal(u1, u2)
+    np.testing.assert_array_equal(c1, c2)
+    np.testing.assert_array_equal(u1, u3)
+    assert s1["irls_iters"] == s2["irls_iters"] == s3["irls_iters"]
+    assert s1["cg_iters_total"] == s2["cg_iters_total"]
+
+
+def test_fixed_iters_runs_every_iteration():
+    # tol = cg_tol = 0: only the numerical breaks can end an iteration early
+    from oracle.irls_oracle import OracleStats
+    p, c, _ = gen_g1(128, 128, seed=8)
+    ost = OracleStats()
+    uo, cco = oracle_unwrap(p, c, max_iter=6, cg_max_iter=7, tol=0.0, cg_tol=0.0, stats=ost)
+    _, _, st = _solve_flags(p, c, 0, max_iter=6, cg_max_iter=7, fixed_iters=True)
+    assert st["irls_iters"] == ost.irls_iters == 6
+    assert st["cg_iters_total"] == sum(ost.cg_iters)
+    u, cc, st = core_b200.irls_unwrap_2d(p, c, max_iter=6, cg_max_iter=7, fixed_iters=True, return_stats=True)
+    assert st["irls_iters"] == 6 and st["cg_iters_total"] == sum(ost.cg_iters)
+    _compare(u, cc, uo, cco, p)
