@@ -82,6 +82,11 @@ SIGNATURES = {
     "unw_apply_preconditioner": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
                                            C.c_size_t, C.c_void_p]),
     "unw_apply_preconditioner_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
+    "unw_adjoint_workspace_bytes": (C.c_size_t, [C.c_int64, C.c_int64]),
+    "unw_adjoint_f32": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
+                                  C.POINTER(UnwParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_size_t,
+                                  C.POINTER(UnwStats), C.c_void_p]),
 }
 
 _lock = threading.Lock()

@@ -1,0 +1,91 @@
+"""Differentiable unwrap: a torch.autograd.Function over the B200 solver.
+
+The forward pass is `irls_unwrap_2d` on CUDA tensors.  The backward pass calls
+`unw_adjoint_f32`: gradients of the unwrap with the forward solution's IRLS
+scale, valid mask, components and median 2-pi shift held fixed (the frozen
+final IRLS system of insardev/insardev/utils_unwrap2d.py:1529-1626 and the
+alignment of :1667-1716), through an implicit adjoint solve with the same
+DCT-preconditioned PCG.  The reference has no differentiable path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import _lib
+from .unwrap2d import _torch, irls_unwrap_2d, make_params
+
+
+def irls_adjoint(phase, weight, u, grad_u, *, cg_max_iter=1000, cg_tol=1e-6, epsilon=1e-2, need_weight=True):
+    """dL/dphase (and dL/dweight) for dL/du = grad_u at the forward output u.
+
+    All arrays are CUDA float32 tensors of one shape.  cg_tol is relative to the
+    initial residual of each of the two PCG solves.  Returns (grad_phase,
+    grad_weight or None, stats dict).
+    """
+    torch = _torch()
+    lib = _lib.load()
+    dev = phase.device
+    H, W = int(phase.shape[0]), int(phase.shape[1])
+    f32 = lambda t: t.detach().to(device=dev, dtype=torch.float32).contiguous()
+    ph, uu, gu = f32(phase), f32(u), f32(grad_u)
+    wt = f32(weight) if weight is not None else None
+    gph = torch.empty((H, W), dtype=torch.float32, device=dev)
+    gw = torch.empty((H, W), dtype=torch.float32, device=dev) if (wt is not None and need_weight) else None
+    ws = torch.empty(lib.unw_adjoint_workspace_bytes(H, W), dtype=torch.uint8, device=dev)
+    prm = make_params(cg_max_iter=cg_max_iter, cg_tol=cg_tol, epsilon=epsilon)
+    st = _lib.UnwStats()
+    with torch.cuda.device(dev):
+        rc = lib.unw_adjoint_f32(ph.data_ptr(), W, wt.data_ptr() if wt is not None else None, W, H, W,
+                                 C.byref(prm), uu.data_ptr(), W, gu.data_ptr(), W, gph.data_ptr(), W,
+                                 gw.data_ptr() if gw is not None else None, W, ws.data_ptr(), ws.numel(),
+                                 C.byref(st), torch.cuda.current_stream(dev).cuda_stream)
+    _lib.check(rc, "unw_adjoint_f32")
+    stats = {"refine_cg_iters": int(st.cg_iters[0]), "adjoint_cg_iters": int(st.cg_iters[1]),
+             "adjoint_rel_residual": float(st.rel_change), "status": int(st.status), "numeric_warning": rc == 1}
+    return gph, gw, stats
+
+
+def _make_function():
+    torch = _torch()
+
+    class _Fn(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, phase, weight, kw, akw):
+            u, cc = irls_unwrap_2d(phase, weight, **kw)
+            ctx.save_for_backward(phase, weight if weight is not None else phase.new_empty(0), u)
+            ctx.has_weight = weight is not None
+            ctx.akw = akw
+            ctx.mark_non_differentiable(cc)
+            return u, cc
+
+        @staticmethod
+        def backward(ctx, grad_u, grad_cc):
+            phase, weight, u = ctx.saved_tensors
+            w = weight if ctx.has_weight else None
+            gph, gw, _ = irls_adjoint(phase, w, u, grad_u, need_weight=ctx.needs_input_grad[1], **ctx.akw)
+            return gph, gw, None, None
+
+    return _Fn
+
+
+_FN = None
+
+
+def irls_unwrap_2d_diff(phase, weight=None, max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2,
+                        conncomp_size=30, *, adjoint_cg_max_iter=1000, adjoint_cg_tol=1e-6):
+    """`irls_unwrap_2d` on CUDA tensors with gradients for phase and weight.
+
+    Returns (u, conncomp); u carries autograd history (conncomp does not).
+    adjoint_cg_max_iter / adjoint_cg_tol control the backward pass's PCG solves
+    (tolerance relative to each solve's initial residual).
+    """
+    global _FN
+    torch = _torch()
+    if not (isinstance(phase, torch.Tensor) and phase.is_cuda):
+        raise ValueError("irls_unwrap_2d_diff takes CUDA tensors")
+    if _FN is None:
+        _FN = _make_function()
+    kw = dict(max_iter=max_iter, tol=tol, cg_max_iter=cg_max_iter, cg_tol=cg_tol, epsilon=epsilon,
+              conncomp_size=conncomp_size)
+    akw = dict(cg_max_iter=adjoint_cg_max_iter, cg_tol=adjoint_cg_tol, epsilon=epsilon)
+    return _FN.apply(phase, weight, kw, akw)

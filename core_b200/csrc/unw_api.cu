@@ -736,6 +736,145 @@ int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, s
     return ret;
 }
 
+// ------------------------------------------------------------ adjoint
+// Workspace of the adjoint: the solver layout of one grid plus a separate
+// post-processing region, since the component labels and sums must live
+// next to the frozen weights (which the forward solve lets them overlay).
+struct AdjLayout {
+    BatchLayout B;
+    size_t parent, lab, csum, adj, ccount, remap, total;
+};
+
+AdjLayout adjoint_layout(long long H, long long W) {
+    AdjLayout A;
+    A.B = batch_layout(1, &H, &W);
+    const long long cap = A.B.g[0].lab_cap;
+    size_t o = up(A.B.total - ALIGN, ALIGN);
+    auto take = [&](size_t bytes) { size_t r = o; o = up(o + bytes, ALIGN); return r; };
+    A.parent = take(sizeof(int) * (size_t)(H * W));
+    A.lab = take(sizeof(int) * (size_t)(H * W));
+    A.csum = take(sizeof(double) * 4 * (size_t)cap);
+    A.adj = take(sizeof(double) * (size_t)cap);
+    A.ccount = take(sizeof(int) * (size_t)cap);
+    A.remap = take(sizeof(int) * (size_t)cap);
+    A.total = o + ALIGN;
+    return A;
+}
+
+int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_t weight_pitch, int64_t H, int64_t W,
+            const unw_params* prm, const float* u, int64_t u_pitch, const float* gu, int64_t gu_pitch, float* gph,
+            int64_t gph_pitch, float* gw, int64_t gw_pitch, void* ws, size_t ws_bytes, unw_stats* stats,
+            cudaStream_t s) {
+    if (!phase || !u || !gu || !gph) return set_err(UNW_E_ARG, "null pointer");
+    if (H <= 0 || W <= 0) return set_err(UNW_E_ARG, "bad shape %lld x %lld", (long long)H, (long long)W);
+    if (H * W >= (1LL << 31)) return set_err(UNW_E_UNSUPPORTED, "too many pixels");
+    if (phase_pitch < W || u_pitch < W || gu_pitch < W || gph_pitch < W || (weight && weight_pitch < W) ||
+        (gw && gw_pitch < W))
+        return set_err(UNW_E_ARG, "pitch smaller than width");
+    if (gw && !weight) return set_err(UNW_E_ARG, "grad_weight needs weight");
+    int rc = validate_params(prm);
+    if (rc) return rc;
+    if (prm->cg_max_iter < 1 || !(prm->cg_tol > 0.f))
+        return set_err(UNW_E_ARG, "adjoint needs cg_max_iter >= 1 and a relative cg_tol > 0");
+    if (!ws) return set_err(UNW_E_ARG, "workspace is NULL");
+    const AdjLayout A = adjoint_layout(H, W);
+    char* base = (char*)up((size_t)ws, ALIGN);
+    if ((size_t)(base - (char*)ws) + A.total - ALIGN > ws_bytes)
+        return set_err(UNW_E_WORKSPACE, "workspace %zu bytes < %zu needed", ws_bytes, A.total);
+    if (stats) memset(stats, 0, sizeof(unw_stats));
+    CK(cudaMemset2DAsync(gph, sizeof(float) * gph_pitch, 0, sizeof(float) * W, H, s));
+    if (gw) CK(cudaMemset2DAsync(gw, sizeof(float) * gw_pitch, 0, sizeof(float) * W, H, s));
+
+    // bounding box of the valid pixels, as in the forward solve
+    const BatchLayout& B = A.B;
+    int* dbbox = (int*)(base + B.bbox);
+    CK(unw_launch_bbox(phase, phase_pitch, (int)H, (int)W, (int*)(base + B.rowany), (int*)(base + B.colany), dbbox,
+                       s));
+    std::vector<int> bbox(4);
+    CK(cudaMemcpyAsync(bbox.data(), dbbox, sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (bbox[1] <= bbox[0] || bbox[3] <= bbox[2]) return UNW_OK;  // all NaN: zero gradients
+
+    unw_grid q{};
+    q.phase = phase;
+    q.phase_pitch = phase_pitch;
+    q.weight = weight;
+    q.weight_pitch = weight_pitch;
+    q.H = H;
+    q.W = W;
+    unw_params pa = *prm;
+    pa.max_iter = 1;
+    pa.flags = 0;
+    Solver S;
+    rc = prepare(S, std::vector<int>{0}, &q, bbox, &pa, base, B, s, false, 0, 0);
+    if (rc) return rc;
+    S.sc.cg_tol = 0.f;            // replaced by cg_rel * ||r0|| at each PCG start
+    S.sc.cg_rel = prm->cg_tol;
+    {
+        GridDev& G = S.hg[0];
+        G.parent = (int*)(base + A.parent);
+        G.lab = (int*)(base + A.lab);
+        G.csum = (double*)(base + A.csum);
+        G.adj = (double*)(base + A.adj);
+        G.ccount = (int*)(base + A.ccount);
+        G.remap = (int*)(base + A.remap);
+        CK(cudaMemcpyAsync(S.dg, S.hg.data(), sizeof(GridDev), cudaMemcpyHostToDevice, s));
+    }
+    const int n = 1;
+    const int ne = S.total[KS_ELEM];
+    CK(unw_launch_simple(UNW_K_STATE_INIT, 1, s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
+    CK(unw_launch_simple(UNW_K_SETUP, ne, s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
+    CK(unw_launch_adj(UNW_A_LOAD, ne, s, S.dg, S.ds(KS_ELEM), n, u, u_pitch, gu, gu_pitch, nullptr, 0, nullptr, 0));
+    // 1. the frozen-weight system at u (IRLS weights and right-hand side from u), solved to
+    //    the relative tolerance from u: u* in U1
+    rc = enqueue_iteration(S, 0);
+    if (rc) return rc;
+    // 2. components of the valid mask and the per-component sin/cos sums at u*
+    const int nt = S.total[KS_NKIND];
+    CK(unw_launch_post(UNW_P_SHIFT_CCINIT, ne, s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+    CK(unw_launch_post(UNW_P_UNION, ne, s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+    CK(unw_launch_post(UNW_P_FLATTEN, nt, s, S.dg, S.ds(KS_NKIND), n, S.sc, S.hg.data()));
+    CK(unw_launch_post(UNW_P_TILESCAN, n, s, S.dg, nullptr, n, S.sc, S.hg.data()));
+    CK(unw_launch_post(UNW_P_LABEL, nt, s, S.dg, S.ds(KS_NKIND), n, S.sc, S.hg.data()));
+    CK(unw_launch_post(UNW_P_ACCUM, ne, s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
+    // 3. adjoint right-hand side through the alignment, then lambda = A^+ G' (x0 = 0, U0)
+    CK(cudaMemsetAsync(S.hg[0].adj, 0, sizeof(double) * (size_t)S.hg[0].lab_cap, s));
+    CK(unw_launch_adj(UNW_A_LSUM, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
+    CK(unw_launch_adj(UNW_A_RHS, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
+    CK(unw_launch_adj(UNW_A_REARM, 1, s, S.dg, nullptr, n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
+    CK(L_rowf(S, 1, 1, 0));
+    CK(L_col(S, 1));
+    CK(L_rowi(S, 1));
+    for (int k = 0; k < S.sc.cg_max_iter; k++) {
+        CK(unw_launch_simple(UNW_K_MATVEC, S.total[KS_MATVEC], s, S.dg, S.ds(KS_MATVEC), n, k, S.sc));
+        CK(L_rowf(S, 2, 1, k));
+        CK(L_col(S, 2));
+        CK(L_rowi(S, 2));
+    }
+    // 4. gradients
+    CK(unw_launch_adj(UNW_A_GRAD, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, gph, gph_pitch, gw,
+                      gw_pitch));
+    std::vector<InstState> hs;
+    rc = read_states(S, hs);
+    if (rc) return rc;
+    const InstState& st = hs[0];
+    if (stats) {
+        unw_stats& o = *stats;
+        o.irls_iters = 1;
+        o.cg_iters[0] = st.cg_log[0];
+        o.cg_iters[1] = st.cg_iter;
+        o.cg_iters_last = st.cg_iter;
+        o.cg_iters_total = st.cg_log[0] + st.cg_iter;
+        o.n_labels = st.n_labels;
+        o.status = st.status;
+        // relative residual of the adjoint solve (cg_tol = cg_rel * ||r0||)
+        o.rel_change = st.cg_tol > 0.f ? st.rnorm * (double)prm->cg_tol / (double)st.cg_tol : 0.0;
+        for (int k = 0; k < 4; k++) o.bbox[k] = bbox[k];
+    }
+    if (!st.irls_active) return UNW_W_NUMERIC;  // non-finite refinement: gradients are zero
+    return UNW_OK;
+}
+
 // Full-grid, dense-pitch descriptor over caller arrays for the operator entry points.
 int op_prepare(Solver& S, int64_t H, int64_t W, void* ws, size_t wsb, cudaStream_t s, const float* phase,
                const float* weight) {
@@ -810,6 +949,21 @@ int unw_solve_f32(const float* phase, int64_t phase_pitch, const float* weight, 
 int unw_solve_batch(int32_t n, const unw_grid* grids, const unw_params* params, void* workspace,
                     size_t workspace_bytes, unw_stats* stats, void* cuda_stream) {
     return solve_batch(n, grids, params, workspace, workspace_bytes, stats, (cudaStream_t)cuda_stream);
+}
+
+size_t unw_adjoint_workspace_bytes(int64_t H, int64_t W) {
+    if (H <= 0 || W <= 0) return 0;
+    return adjoint_layout(H, W).total;
+}
+
+int unw_adjoint_f32(const float* phase, int64_t phase_pitch, const float* weight, int64_t weight_pitch, int64_t H,
+                    int64_t W, const unw_params* params, const float* u, int64_t u_pitch, const float* grad_u,
+                    int64_t grad_u_pitch, float* grad_phase, int64_t grad_phase_pitch, float* grad_weight,
+                    int64_t grad_weight_pitch, void* workspace, size_t workspace_bytes, unw_stats* stats,
+                    void* cuda_stream) {
+    return adjoint(phase, phase_pitch, weight, weight_pitch, H, W, params, u, u_pitch, grad_u, grad_u_pitch,
+                   grad_phase, grad_phase_pitch, grad_weight, grad_weight_pitch, workspace, workspace_bytes, stats,
+                   (cudaStream_t)cuda_stream);
 }
 
 int unw_setup_gradients(const float* phase, const float* weight, int64_t H, int64_t W, float* gx, float* gy,

@@ -72,6 +72,7 @@ __device__ __forceinline__ float4 rowf_vals4(const GridDev& G, float* __restrict
             const float val = fsub(f4get(b4, q), -res);
             out[q] = val;
             acc[0] += isfinite(val) ? 0.0 : 1.0;
+            acc[1] += (double)val * (double)val;
         }
         const float4 r4 = make_float4(out[0], out[1], out[2], out[3]);
         st4f(G.r, o, r4);

@@ -60,6 +60,7 @@ struct InstState {
     double best_residual;
     double rel_change;
     float tol, cg_tol, eps2;
+    float cg_rel;               // > 0: cg_tol = cg_rel * ||r0|| at the PCG start
     int cg_max_iter;
     int cg_total;
     int cg_log[UNW_MAX_LOG];

@@ -10,6 +10,7 @@ struct UnwScalars {
     float cg_tol;
     float eps2;
     int conncomp_size;
+    float cg_rel;     // > 0: PCG tolerance relative to the initial residual norm (adjoint solves)
 };
 
 enum {
@@ -70,3 +71,15 @@ enum {
 };
 cudaError_t unw_launch_post(int which, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
                             int n, const UnwScalars& sc, const GridDev* host_grids);
+
+// frozen-weight adjoint (KS_ELEM shapes except REARM)
+enum {
+    UNW_A_LOAD = 0,     // forward output and dL/dout into the crop
+    UNW_A_LSUM,         // per-component sum of dL/dout
+    UNW_A_RHS,          // adjoint right-hand side, x0 = 0
+    UNW_A_REARM,        // solver state for the adjoint PCG
+    UNW_A_GRAD          // dL/dphase, dL/dweight
+};
+cudaError_t unw_launch_adj(int which, int nblk, cudaStream_t s, const GridDev* gd, const int* starts, int n,
+                           const float* a, long long ap, const float* b, long long bp, float* c, long long cp,
+                           float* d, long long dp);

@@ -50,6 +50,7 @@ __device__ __forceinline__ float rowfwd_value(const GridDev& G, float* __restric
         const float val = fsub(G.b[o], ax);
         G.r[o] = val;
         acc[0] += isfinite(val) ? 0.0 : 1.0;
+        acc[1] += (double)val * (double)val;
         return val;
     } else {
         const float xn = fmaf(alpha, pk[o], U[o]);
@@ -67,6 +68,7 @@ __device__ __forceinline__ void rowfwd_finalize(InstState* st, const double (&ac
     if (MODE == 1) {
         // non-finite initial residual: CG returns x0 (utils_unwrap2d.py:1418-1419)
         st->cg_active = acc[0] == 0.0 ? 1 : 0;
+        if (st->cg_rel > 0.f) st->cg_tol = (float)((double)st->cg_rel * sqrt(acc[1]));
     } else if (MODE == 2) {
         const double rn = sqrt(acc[0]);
         st->rnorm = rn;

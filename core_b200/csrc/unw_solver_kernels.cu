@@ -79,6 +79,7 @@ __global__ void k_state_init(const GridDev* __restrict__ grids, int n, UnwScalar
     s->best_update = 0; s->revert = 0; s->u_index = 0; s->status = 0;
     s->vcount = 0; s->mean = 0; s->residual = 0; s->best_residual = INFINITY; s->rel_change = 0;
     s->tol = sc.tol; s->cg_tol = sc.cg_tol; s->eps2 = sc.eps2; s->cg_max_iter = sc.cg_max_iter;
+    s->cg_rel = sc.cg_rel;
     s->cg_total = 0;
     for (int i = 0; i < UNW_MAX_LOG; i++) s->cg_log[i] = 0;
     s->n_nonfinite = 0; s->kmin = INT_MAX; s->kmax = INT_MIN; s->hist_ok = 1; s->kmed = 0.f; s->shift = 0.f;

@@ -158,6 +158,42 @@ UNW_API int unw_apply_preconditioner(const float* r, int64_t H, int64_t W, float
                              void* workspace, size_t workspace_bytes, void* cuda_stream);
 
 /*
+ * Gradients through the unwrap (frozen-weight implicit adjoint).  It has no
+ * counterpart in the reference, whose solve is not differentiable.
+ *
+ * The differentiated map is the unwrap with what the forward solution fixes
+ * held constant: the valid mask, its 4-connected components, the median
+ * 2-pi shift and the IRLS scale 1/sqrt(r^2 + eps^2) of every edge at u
+ * (utils_unwrap2d.py:1560-1574).  What remains is differentiable: the wrapped
+ * phase differences, the coherence edge weights, the weighted Poisson solve
+ * A(wI) u* = b (utils_unwrap2d.py:1367-1388, :1576-1581) and the per-component
+ * circular-mean alignment (utils_unwrap2d.py:1694-1716).  The call first
+ * refines u to u* on that frozen system, then solves the adjoint system with
+ * the same DCT-preconditioned PCG, then forms the gradients.
+ *   phase, weight   the forward call's inputs (device, NaN = invalid)
+ *   u               the forward call's unwrapped output (device)
+ *   grad_u          dL/du (device; ignored where phase is NaN)
+ *   params          epsilon as in the forward call; cg_max_iter caps each of
+ *                   the two PCG solves; cg_tol is RELATIVE to the initial
+ *                   residual norm of each solve (e.g. 1e-6)
+ *   grad_phase      dL/dphase (device), 0 where phase is NaN
+ *   grad_weight     dL/dweight (device) or NULL; needs weight
+ *   stats           cg_iters[0] / [1]: refinement / adjoint PCG iterations,
+ *                   rel_change: final relative residual of the adjoint solve
+ * Returns UNW_W_NUMERIC (gradients 0) when the refinement is not finite.
+ */
+UNW_API size_t unw_adjoint_workspace_bytes(int64_t H, int64_t W);
+UNW_API int unw_adjoint_f32(const float* phase, int64_t phase_pitch,
+                            const float* weight, int64_t weight_pitch,
+                            int64_t H, int64_t W, const unw_params* params,
+                            const float* u, int64_t u_pitch,
+                            const float* grad_u, int64_t grad_u_pitch,
+                            float* grad_phase, int64_t grad_phase_pitch,
+                            float* grad_weight, int64_t grad_weight_pitch,
+                            void* workspace, size_t workspace_bytes,
+                            unw_stats* stats, void* cuda_stream);
+
+/*
  * Allocation-free variant of unw_apply_preconditioner.  It has no counterpart
  * in the reference.  It is for callers that cannot allocate device memory
  * where they need the operator (inside another framework's graph capture or

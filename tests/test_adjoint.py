@@ -1,0 +1,114 @@
+"""Frozen-weight adjoint (unw_adjoint_f32, core_b200.irls_unwrap_2d_diff).
+
+The FP64 oracle (oracle/adjoint_oracle.py) restates the differentiated map
+and its adjoint; the CPU tests pin the oracle's adjoint against central finite
+differences of the map itself, the GPU tests compare the CUDA adjoint with the
+oracle's (and with finite differences) on the same inputs and the same
+forward solution.
+
+Tolerances, relative to the largest gradient: oracle vs finite differences
+1e-4 (h = 1e-5 phase, 1e-6 weight); CUDA (float32 PCG solves to 1e-6 relative
+residual) vs the oracle 1e-4 for dL/dphase and dL/dweight, and vs finite
+differences 1e-4.
+"""
+import numpy as np
+import pytest
+
+from oracle.adjoint_oracle import Frozen
+from oracle.generators import gen_g1
+from oracle.irls_oracle import irls_unwrap_2d as oracle_unwrap
+
+
+def _split_nan(p, c):
+    """A NaN column band that splits the grid into two components, plus the generator's blobs."""
+    p = p.copy(); c = c.copy()
+    W = p.shape[1]
+    p[:, W // 2:W // 2 + 2] = np.nan
+    c[:, W // 2:W // 2 + 2] = np.nan
+    return p, c
+
+
+def _case(kind, H=24, W=28, seed=3):
+    p, c, t = gen_g1(H, W, seed=seed, noise=1.2, nan_fraction=0.0 if kind == "full" else 0.05)
+    if kind == "split":
+        p, c = _split_nan(p, c)
+    return p, c
+
+
+def _relerr(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+
+
+@pytest.mark.parametrize("kind", ["full", "nan", "split"])
+def test_oracle_adjoint_matches_finite_differences(kind):
+    p, c = _case(kind)
+    u, _ = oracle_unwrap(p, c, dtype=np.float64)
+    F = Frozen(p, c, u)
+    v = np.isfinite(p)
+    rng = np.random.default_rng(1)
+    G = np.where(v, rng.standard_normal(p.shape), np.nan)
+    gp, gw = F.adjoint(p, c, G)
+    pix = [tuple(x) for x in np.argwhere(v)[rng.choice(v.sum(), 24, replace=False)]]
+    fdp = F.finite_difference(p, c, G, pix, h=1e-5)
+    fdw = F.finite_difference(p, c, G, pix, h=1e-6, wrt="weight")
+    assert _relerr(np.array([gp[i, j] for i, j in pix]), fdp) <= 1e-4
+    assert _relerr(np.array([gw[i, j] for i, j in pix]), fdw) <= 1e-4
+    assert (gp[~v] == 0).all() and (gw[~v] == 0).all()
+    if kind == "split":
+        assert F.nlab >= 2
+
+
+# ------------------------------------------------------------------ GPU
+def _gpu():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["full", "nan", "split"])
+def test_cuda_adjoint_matches_oracle(kind):
+    torch = _gpu()
+    import core_b200
+    p, c = _case(kind, H=40, W=48, seed=5)
+    dev = torch.device("cuda", 0)
+    u, _ = core_b200.irls_unwrap_2d(p, c)
+    v = np.isfinite(p)
+    rng = np.random.default_rng(2)
+    G = np.where(v, rng.standard_normal(p.shape), np.nan).astype(np.float32)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+    gph, gw, st = core_b200.irls_adjoint(T(p), T(c), T(u), T(G), cg_max_iter=3000, cg_tol=1e-6)
+    gph, gw = gph.cpu().numpy(), gw.cpu().numpy()
+    assert st["adjoint_rel_residual"] <= 1e-6 and not st["numeric_warning"]
+    F = Frozen(p, c, u)
+    op, ow = F.adjoint(p, c, G)
+    assert (gph[~v] == 0).all() and (gw[~v] == 0).all()
+    assert _relerr(gph, op) <= 1e-4, _relerr(gph, op)
+    assert _relerr(gw, ow) <= 1e-4, _relerr(gw, ow)
+    pix = [tuple(x) for x in np.argwhere(v)[rng.choice(v.sum(), 16, replace=False)]]
+    fdp = F.finite_difference(p, c, G, pix, h=1e-5)
+    assert _relerr(np.array([gph[i, j] for i, j in pix]), fdp) <= 1e-4
+
+
+@pytest.mark.gpu
+def test_autograd_function_backward():
+    torch = _gpu()
+    import core_b200
+    p, c, truth = gen_g1(64, 72, seed=7, noise=1.0)
+    dev = torch.device("cuda", 0)
+    pt = torch.from_numpy(p).to(dev).requires_grad_(True)
+    ct = torch.from_numpy(c).to(dev).requires_grad_(True)
+    tt = torch.from_numpy(truth.astype(np.float32)).to(dev)
+    u, cc = core_b200.irls_unwrap_2d_diff(pt, ct)
+    v = torch.isfinite(u)
+    loss = 0.5 * (u[v] - tt[v]).pow(2).sum()
+    loss.backward()
+    assert pt.grad is not None and ct.grad is not None
+    assert torch.isfinite(pt.grad).all() and torch.isfinite(ct.grad).all()
+    assert (pt.grad[~v] == 0).all()
+    # the same gradients through the direct call
+    G = torch.where(v, u - tt, torch.zeros_like(u)).detach()
+    gph, gw, _ = core_b200.irls_adjoint(pt.detach(), ct.detach(), u.detach(), G)
+    assert torch.allclose(pt.grad, gph, rtol=0, atol=1e-6 * float(gph.abs().max()))
+    assert torch.allclose(ct.grad, gw, rtol=0, atol=1e-6 * float(gw.abs().max()) + 1e-30)

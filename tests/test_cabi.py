@@ -74,3 +74,24 @@ def test_python_boundary_validation_without_gpu():
         core_b200.irls_unwrap_2d(np.zeros((4, 4), np.float32), device="cpu")
     with pytest.raises(ValueError):
         core_b200.irls_unwrap_2d(np.zeros((4, 4), np.float32), device="mps")
+
+
+def test_adjoint_rejects_bad_args_without_gpu():
+    lib = _lib.load()
+    prm = _lib.UnwParams(50, 1e-3, 200, 1e-6, 1e-2, 30, 0, 1)
+    f = C.c_void_p(0x10000)
+    big = 1 << 40
+    assert lib.unw_adjoint_workspace_bytes(64, 64) > lib.unw_workspace_bytes(64, 64)
+    assert lib.unw_adjoint_workspace_bytes(0, 64) == 0
+    call = lambda *a: lib.unw_adjoint_f32(*a)
+    rc = call(None, 8, None, 8, 8, 8, C.byref(prm), f, 8, f, 8, f, 8, None, 8, f, big, None, None)
+    assert rc == _lib.UNW_E_ARG and "null" in _lib.last_error()
+    rc = call(f, 8, None, 8, 8, 8, C.byref(prm), f, 4, f, 8, f, 8, None, 8, f, big, None, None)
+    assert rc == _lib.UNW_E_ARG and "pitch" in _lib.last_error()
+    rc = call(f, 8, None, 8, 8, 8, C.byref(prm), f, 8, f, 8, f, 8, f, 8, f, big, None, None)
+    assert rc == _lib.UNW_E_ARG and "weight" in _lib.last_error()
+    rel0 = _lib.UnwParams(50, 1e-3, 200, 0.0, 1e-2, 30, 0, 1)
+    rc = call(f, 8, None, 8, 8, 8, C.byref(rel0), f, 8, f, 8, f, 8, None, 8, f, big, None, None)
+    assert rc == _lib.UNW_E_ARG and "relative" in _lib.last_error()
+    rc = call(f, 8, None, 8, 8, 8, C.byref(prm), f, 8, f, 8, f, 8, None, 8, f, 64, None, None)
+    assert rc == _lib.UNW_E_WORKSPACE
