@@ -73,6 +73,19 @@ long long next_smooth(long long x) {
     return x;
 }
 int fft_len(int N) { return smooth7(N) ? N : (int)next_smooth(2LL * N - 1); }
+long long next_pow2(long long x) {
+    long long p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+// Bluestein length M (power of two >= 2N - 1, >= 256) of the register-FFT path
+// for a DCT length N that is not a power of two; 0 where that path is not used
+// (powers of two have their own kernels; very short axes stay on the generic
+// shared-memory FFT; N > 8192 would need M > 16384).
+int bl_len(int N) {
+    if (N <= 64 || 2LL * N - 1 > MAX_FFT || (N & (N - 1)) == 0) return 0;
+    return (int)std::max<long long>(256, next_pow2(2LL * N - 1));
+}
 
 std::vector<int> factor(int n) {
     std::vector<int> r;
@@ -106,8 +119,9 @@ struct HostPlan {
 HostPlan make_plan(int N) {
     HostPlan p;
     p.N = N;
-    p.blue = smooth7(N) ? 0 : 1;
-    p.n = fft_len(N);
+    const int M = bl_len(N);
+    p.blue = (M || !smooth7(N)) ? 1 : 0;
+    p.n = M ? M : fft_len(N);
     p.rad = p.n > 1 ? factor(p.n) : std::vector<int>{};
     p.cap = plan_cap(p.rad);
     return p;
@@ -139,8 +153,14 @@ GridLayout grid_layout(long long H0, long long W0) {
     const size_t A = (size_t)H0 * (size_t)L.P0 * sizeof(float);
     L.max_ctas = std::max<long long>({(H0 + 1) / 2, (W0 + 1) / 2, ((W0 + 127) / 128) * ((H0 + 7) / 8),
                                       ELEM_MAX_CTAS});
-    L.fr_cap = (int)std::max<long long>(next_smooth(2 * W0 - 1), W0);
-    L.fc_cap = (int)std::max<long long>(next_smooth(2 * H0 - 1), H0);
+    // room for the longest transform of any crop: Bluestein lengths (smooth or
+    // power of two, see bl_len) and direct lengths
+    auto cap = [](long long N0) {
+        long long c = std::max<long long>(next_smooth(2 * N0 - 1), N0);
+        return std::max<long long>(c, std::min<long long>(MAX_FFT, std::max<long long>(256, next_pow2(2 * N0 - 1))));
+    };
+    L.fr_cap = (int)cap(W0);
+    L.fc_cap = (int)cap(H0);
     L.st = take(sizeof(InstState));
     L.counter = take(sizeof(unsigned) * 4);
     L.part = take((size_t)L.max_ctas * UNW_NPART * sizeof(double));
@@ -200,6 +220,7 @@ struct Shape {
     int row_T = 0, col_T = 0;
     size_t row_smem = 0, col_smem = 0;
     int row_p2 = 0, col_p2 = 0;   // power-of-two register-FFT paths (length), 0 = generic
+    int row_bl = 0, col_bl = 0;   // Bluestein register-FFT paths (FFT length M), 0 = not used
 };
 
 int elem_ctas(long long npx) {
@@ -284,16 +305,20 @@ int kind_ctas(const GridDev& G, int kind) {
 cudaError_t L_rowf(Solver& S, int mode, int it, int cgk) {
     if (S.sh.row_p2)
         return unw_launch_rowf_p2(S.sh.row_p2, mode, S.total[KS_ROWPAIR], S.s, S.dg, S.ds(KS_ROWPAIR), S.n, it, cgk);
+    if (S.sh.row_bl)
+        return unw_launch_rowf_bl(S.sh.row_bl, mode, S.total[KS_ROWPAIR], S.s, S.dg, S.ds(KS_ROWPAIR), S.n, it, cgk);
     return unw_launch_row_fwd(mode, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg,
                               S.ds(KS_ROWPAIR), S.n, it, cgk);
 }
 cudaError_t L_rowi(Solver& S, int mode) {
     if (S.sh.row_p2) return unw_launch_rowi_p2(S.sh.row_p2, mode, S.total[KS_ROWPAIR], S.s, S.dg, S.ds(KS_ROWPAIR), S.n);
+    if (S.sh.row_bl) return unw_launch_rowi_bl(S.sh.row_bl, mode, S.total[KS_ROWPAIR], S.s, S.dg, S.ds(KS_ROWPAIR), S.n);
     return unw_launch_row_inv(mode, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg,
                               S.ds(KS_ROWPAIR), S.n);
 }
 cudaError_t L_col(Solver& S, int mode) {
     if (S.sh.col_p2) return unw_launch_col_p2(S.sh.col_p2, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n);
+    if (S.sh.col_bl) return unw_launch_col_bl(S.sh.col_bl, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n);
     return unw_launch_col(mode, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, S.s, S.dg, S.ds(KS_COL), S.n);
 }
 
@@ -394,8 +419,10 @@ std::array<int, 4> group_key(int H, int W) {
     auto p2 = [](int n) { return n >= 256 && n <= MAX_FFT && (n & (n - 1)) == 0; };
     std::array<int, 4> k{};
     if (p2(W)) { k[0] = 1; k[1] = W; }
+    else if (bl_len(W)) { k[0] = 2; k[1] = bl_len(W); }
     else { const HostPlan hp = make_plan(W); k[0] = 0; k[1] = pick_threads(hp.n, hp.cap); }
     if (p2(H)) { k[2] = 1; k[3] = H; }
+    else if (bl_len(H)) { k[2] = 2; k[3] = bl_len(H); }
     else {
         const HostPlan hp = make_plan(H);
         int nseq = col_nseq_generic(hp.n, W), cT = 0;
@@ -521,8 +548,25 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
             S.sh.col_p2 = h;
             for (int g = 0; g < n; g++) S.hg[g].col_nseq = unw_p2_col_nseq(h);
         }
+        // Bluestein register-FFT paths when every grid has the same M along the axis
+        int mw = -1, mh = -1;
+        bool mwsame = true, mhsame = true;
+        for (int g = 0; g < n; g++) {
+            const GridDev& G = S.hg[g];
+            if (G.H == 0) continue;
+            const int a = bl_len(G.W), b = bl_len(G.H);
+            if (mw < 0) mw = a; else mwsame &= (mw == a);
+            if (mh < 0) mh = b; else mhsame &= (mh == b);
+        }
+        if (!S.sh.row_p2 && mw > 0 && mwsame) S.sh.row_bl = mw;
+        if (!S.sh.col_p2 && mh > 0 && mhsame) {
+            S.sh.col_bl = mh;
+            for (int g = 0; g < n; g++) S.hg[g].col_nseq = unw_bl_col_nseq(mh);
+        }
         // persistent column pass: as many CTAs as fit on the SMs (<= 2048 threads, 4 CTAs)
-        const int cthreads = S.sh.col_p2 ? S.sh.col_p2 / 16 * unw_p2_col_nseq(S.sh.col_p2) : S.sh.col_T;
+        const int cthreads = S.sh.col_p2 ? S.sh.col_p2 / 16 * unw_p2_col_nseq(S.sh.col_p2)
+                             : S.sh.col_bl ? S.sh.col_bl / 16 * unw_bl_col_nseq(S.sh.col_bl)
+                                           : S.sh.col_T;
         const int per_sm = std::max(1, std::min(4, 2048 / std::max(cthreads, 1)));
         for (int g = 0; g < n; g++) S.hg[g].col_ctas = NUM_SMS * per_sm;
     }

@@ -1,0 +1,175 @@
+// Row DCT passes for row lengths N that are not powers of two (64 < N <= 8192):
+// the same row-pair structure as the power-of-two kernels (two real rows are
+// one complex sequence, Makhoul's reordering is a scatter/gather through
+// shared memory), with the length-N DFT done by Bluestein on the register FFT
+// of length M = the power of two >= 2N - 1 (unw_bluestein.cuh).  M / 16
+// threads per CTA; the CTA loops over row pairs.
+#include "unw_bluestein.cuh"
+#include "unw_rowops.cuh"
+#include "unw_kernels.h"
+
+namespace {
+
+template <int T>
+constexpr int bl_min_blocks() { return T >= 1024 ? 1 : (1024 / T > 16 ? 16 : 1024 / T); }
+
+template <int M, int MODE>
+__global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowf_bl(const GridDev* __restrict__ grids,
+                                                                             const int* __restrict__ starts, int n,
+                                                                             int it, int cgk) {
+    constexpr int T = M / 16;
+    extern __shared__ float2 sm[];
+    __shared__ double red[32 * 2];
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    InstState* st = G.st;
+    if (!rowfwd_gate<MODE>(st)) return;
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int H = G.H, W = G.W, P = G.P;
+    const int t = threadIdx.x;
+    float* U = (it & 1) ? G.U0 : G.U1;
+    const float* pk = (MODE == 2) ? G.p0 : nullptr;
+    const float alpha = (MODE == 2) ? st->alpha : 0.f;
+    const float2* __restrict__ dw = G.prow.dctw;
+    double acc[2] = {0.0, 0.0};
+    for (int pair = local; pair < (H + 1) / 2; pair += nct) {
+        const int i0 = 2 * pair, i1 = i0 + 1;
+        const bool has1 = i1 < H;
+        __syncthreads();  // previous row pair's reads of sm are done
+        for (int j = t; j < W; j += T) {
+            const float a = rowfwd_value<MODE>(G, U, pk, alpha, i0, j, acc);
+            const float b = has1 ? rowfwd_value<MODE>(G, U, pk, alpha, i1, j, acc) : 0.f;
+            sm[pad16(mk_perm(j, W))] = make_float2(a, b);
+        }
+        __syncthreads();
+        blue_fft<M>(sm, t, W, G.prow);
+        // two real rows from one complex DFT, then X_k = Re(exp(-i pi k/2W) V_k)
+        float* __restrict__ Ta = G.T + (size_t)i0 * P;
+        float* __restrict__ Tb = G.T + (size_t)i1 * P;
+        for (int k = t; k < W; k += T) {
+            const float2 C = sm[pad16(k)];
+            const float2 Cm = sm[pad16(k == 0 ? 0 : W - k)];
+            const float2 w = __ldg(&dw[k]);
+            const float2 Va = make_float2(C.x + Cm.x, C.y - Cm.y);
+            const float2 Vb = make_float2(C.y + Cm.y, Cm.x - C.x);
+            Ta[k] = w.x * Va.x - w.y * Va.y;
+            if (has1) Tb[k] = w.x * Vb.x - w.y * Vb.y;
+        }
+    }
+    if (MODE == 0 || MODE == 3) return;
+    if (arrive<2>(G, local, nct, acc, red)) {
+        finish_sum<2>(G, nct, acc, red);
+        if (threadIdx.x == 0) rowfwd_finalize<MODE>(st, acc);
+    }
+}
+
+template <int M, int MODE>
+__global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowi_bl(const GridDev* __restrict__ grids,
+                                                                             const int* __restrict__ starts, int n) {
+    constexpr int T = M / 16;
+    extern __shared__ float2 sm[];
+    __shared__ double red[32 * 2];
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    InstState* st = G.st;
+    if (!rowinv_gate<MODE>(st)) return;
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int H = G.H, W = G.W, P = G.P;
+    const int t = threadIdx.x;
+    const float2* __restrict__ dw = G.prow.dctw;
+    const float beta = MODE == 2 ? st->beta : 0.f;
+    double acc[2] = {0.0, 0.0};
+    for (int pair = local; pair < (H + 1) / 2; pair += nct) {
+        const int i0 = 2 * pair, i1 = i0 + 1;
+        const bool has1 = i1 < H;
+        const float* __restrict__ Ta = G.T + (size_t)i0 * P;
+        const float* __restrict__ Tb = G.T + (size_t)i1 * P;
+        __syncthreads();  // previous row pair's reads of sm are done
+        // DCT-III pre-twiddle: V'_k = conj(w_k) (Y_k - i Y_{W-k}), Y_W = 0; store conj(C')
+        for (int k = t; k < W; k += T) {
+            const float ya = Ta[k], yb = has1 ? Tb[k] : 0.f;
+            const float yam = k ? Ta[W - k] : 0.f;
+            const float ybm = (k && has1) ? Tb[W - k] : 0.f;
+            const float2 wc = cconj(__ldg(&dw[k]));
+            const float2 Pa = cmul(wc, make_float2(ya, -yam));
+            const float2 Pb = cmul(wc, make_float2(yb, -ybm));
+            sm[pad16(k)] = cconj(make_float2(Pa.x - Pb.y, Pa.y + Pb.x));
+        }
+        __syncthreads();
+        blue_fft<M>(sm, t, W, G.prow);
+        for (int j = t; j < W; j += T) {
+            const float2 v = sm[pad16(mk_perm(j, W))];
+            rowinv_store<MODE>(G, i0, j, v.x, beta, acc);
+            if (has1) rowinv_store<MODE>(G, i1, j, -v.y, beta, acc);
+        }
+    }
+    if (MODE != 0) return;
+    if (arrive<2>(G, local, nct, acc, red)) {
+        finish_sum<2>(G, nct, acc, red);
+        if (threadIdx.x == 0) rowinv_finalize_initu(st, acc);
+    }
+}
+
+template <int M>
+cudaError_t rowf_bl_m(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* st, int n, int it, int cgk) {
+    const size_t smem = sizeof(float2) * RegFft<M>::SMEM;
+    auto go = [&](auto kfn) {
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kfn<<<nblk, M / 16, smem, s>>>(gd, st, n, it, cgk);
+        return cudaGetLastError();
+    };
+    switch (mode) {
+        case 0: return go(k_rowf_bl<M, 0>);
+        case 1: return go(k_rowf_bl<M, 1>);
+        case 2: return go(k_rowf_bl<M, 2>);
+        default: return go(k_rowf_bl<M, 3>);
+    }
+}
+
+template <int M>
+cudaError_t rowi_bl_m(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* st, int n) {
+    const size_t smem = sizeof(float2) * RegFft<M>::SMEM;
+    auto go = [&](auto kfn) {
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kfn<<<nblk, M / 16, smem, s>>>(gd, st, n);
+        return cudaGetLastError();
+    };
+    switch (mode) {
+        case 0: return go(k_rowi_bl<M, 0>);
+        case 1: return go(k_rowi_bl<M, 1>);
+        case 2: return go(k_rowi_bl<M, 2>);
+        default: return go(k_rowi_bl<M, 3>);
+    }
+}
+
+}  // namespace
+
+#define UNW_BL_SWITCH(M, CALL)                 \
+    switch (M) {                               \
+        case 256: return CALL(256);            \
+        case 512: return CALL(512);            \
+        case 1024: return CALL(1024);          \
+        case 2048: return CALL(2048);          \
+        case 4096: return CALL(4096);          \
+        case 8192: return CALL(8192);          \
+        case 16384: return CALL(16384);        \
+        default: return cudaErrorInvalidValue; \
+    }
+
+cudaError_t unw_launch_rowf_bl(int M, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
+                               int n, int it, int cgk) {
+    if (nblk <= 0) return cudaSuccess;
+#define CALL(MM) rowf_bl_m<MM>(mode, nblk, s, gd, starts, n, it, cgk)
+    UNW_BL_SWITCH(M, CALL)
+#undef CALL
+}
+
+cudaError_t unw_launch_rowi_bl(int M, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
+                               int n) {
+    if (nblk <= 0) return cudaSuccess;
+#define CALL(MM) rowi_bl_m<MM>(mode, nblk, s, gd, starts, n)
+    UNW_BL_SWITCH(M, CALL)
+#undef CALL
+}

@@ -50,6 +50,15 @@ cudaError_t unw_launch_rowi_p2(int N, int mode, int nblk, cudaStream_t s, const 
 cudaError_t unw_launch_col_p2(int N, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
                               int n);
 
+// Bluestein-on-register-FFT DCT passes for other lengths (M = power of two >= 2N - 1)
+int unw_bl_col_nseq(int M);
+cudaError_t unw_launch_rowf_bl(int M, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
+                               int n, int it, int cgk);
+cudaError_t unw_launch_rowi_bl(int M, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
+                               int n);
+cudaError_t unw_launch_col_bl(int M, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
+                              int n);
+
 // bounding box of valid pixels on the caller's full grid
 cudaError_t unw_launch_bbox(const float* phase, long long pitch, int H0, int W0, int* rowany,
                             int* colany, int* bbox, cudaStream_t s);
