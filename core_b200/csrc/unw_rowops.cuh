@@ -153,10 +153,12 @@ __device__ __forceinline__ void col_spectral_pair(float2 C, float2 Cm, int k, in
     const float2 Vbm = make_float2(Vbk.x, -Vbk.y);
     const float xak = wk.x * Vak.x - wk.y * Vak.y, xbk = wk.x * Vbk.x - wk.y * Vbk.y;
     const float xam = wm.x * Vam.x - wm.y * Vam.y, xbm = wm.x * Vbm.x - wm.y * Vbm.y;
-    const float Xak = (k == 0 && ja0) ? 0.f : xak * __frcp_rn(-(ck + ca)) * negs;
-    const float Xam = (km == 0 && ja0) ? 0.f : xam * __frcp_rn(-(cm + ca)) * negs;
-    const float Xbk = hasb ? xbk * __frcp_rn(-(ck + cb)) * negs : 0.f;
-    const float Xbm = hasb ? xbm * __frcp_rn(-(cm + cb)) * negs : 0.f;
+    // X * (negs / lambda), lambda = -(sH + sW) in (-8, 0): a fast division (2 ulp),
+    // well inside the preconditioner's tolerance
+    const float Xak = (k == 0 && ja0) ? 0.f : xak * __fdividef(negs, -(ck + ca));
+    const float Xam = (km == 0 && ja0) ? 0.f : xam * __fdividef(negs, -(cm + ca));
+    const float Xbk = hasb ? xbk * __fdividef(negs, -(ck + cb)) : 0.f;
+    const float Xbm = hasb ? xbm * __fdividef(negs, -(cm + cb)) : 0.f;
     if (RZ) {
         const float ea = ja0 ? 0.5f : 1.0f;
         float tk = fmaf(xak * ea, Xak, xbk * Xbk);
