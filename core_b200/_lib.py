@@ -83,6 +83,10 @@ SIGNATURES = {
                                            C.c_size_t, C.c_void_p]),
     "unw_apply_preconditioner_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "unw_adjoint_workspace_bytes": (C.c_size_t, [C.c_int64, C.c_int64]),
+    "unw_goldstein_workspace_bytes": (C.c_size_t, [C.c_int64, C.c_int64, C.c_int32, C.c_int32]),
+    "unw_goldstein_c64": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
+                                    C.c_int32, C.c_int32, C.c_float, C.c_void_p, C.c_int64, C.c_void_p,
+                                    C.c_size_t, C.c_void_p]),
     "unw_adjoint_f32": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
                                   C.POINTER(UnwParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
                                   C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_size_t,

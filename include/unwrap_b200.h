@@ -194,6 +194,24 @@ UNW_API int unw_adjoint_f32(const float* phase, int64_t phase_pitch,
                             unw_stats* stats, void* cuda_stream);
 
 /*
+ * Goldstein adaptive phase filter on one grid.  Replaces the GPU path of
+ * insardev's filter, goldstein_pytorch (utils_goldstein.py:157-330, dispatched
+ * from Batch.py:2023-2027): psize_y x psize_x patches at half-patch steps,
+ * spectrum weighted by max(|F|, 1e-10)^alpha, alpha = 1 - taper-weighted mean
+ * coherence, taper and overlap-add divided by the number of valid patches
+ * (a patch is valid with at least int(psize_y * psize_x * threshold) non-NaN
+ * pixels); NaN where the input is NaN or no valid patch covers the pixel.
+ *   phase [H][phase_pitch] interleaved complex64 (device), corr [H][corr_pitch]
+ *   float32 (device, NaN allowed), out [H][out_pitch] complex64 (device).
+ * Patch sizes: powers of two in [4, 64] (UNW_E_UNSUPPORTED otherwise).
+ */
+UNW_API size_t unw_goldstein_workspace_bytes(int64_t H, int64_t W, int32_t psize_y, int32_t psize_x);
+UNW_API int unw_goldstein_c64(const float* phase, int64_t phase_pitch, const float* corr, int64_t corr_pitch,
+                              int64_t H, int64_t W, int32_t psize_y, int32_t psize_x, float threshold,
+                              float* out, int64_t out_pitch, void* workspace, size_t workspace_bytes,
+                              void* cuda_stream);
+
+/*
  * Allocation-free variant of unw_apply_preconditioner.  It has no counterpart
  * in the reference.  It is for callers that cannot allocate device memory
  * where they need the operator (inside another framework's graph capture or
