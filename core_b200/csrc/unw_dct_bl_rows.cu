@@ -13,6 +13,43 @@ namespace {
 template <int T>
 constexpr int bl_min_blocks() { return T >= 1024 ? 1 : (1024 / T > 16 ? 16 : 1024 / T); }
 
+__device__ __forceinline__ float4 ld4v(const float* __restrict__ a, size_t o) {
+    return *reinterpret_cast<const float4*>(a + o);
+}
+__device__ __forceinline__ void st4v(float* __restrict__ a, size_t o, float4 v) {
+    *reinterpret_cast<float4*>(a + o) = v;
+}
+__device__ __forceinline__ float f4at(const float4& v, int c) {
+    return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
+}
+
+// x += alpha p, r -= alpha Ap at columns j..j+3 of row i (the reference's PCG
+// update, utils_unwrap2d.py:1445-1459, same operations as rowfwd_value mode 2).
+// Rows are 128-byte aligned with a pitch of whole float4 groups, so a group
+// starting below W stays inside the row; columns >= W are updated but do not
+// enter the norms.
+__device__ __forceinline__ float4 upd4(const GridDev& G, float* __restrict__ U, const float* __restrict__ pk,
+                                       float alpha, int i, int j, int W, double (&acc)[2]) {
+    const size_t o = (size_t)i * G.P + j;
+    const float4 x = ld4v(U, o), p = ld4v(pk, o), r = ld4v(G.r, o), ap = ld4v(G.Ap, o);
+    float4 xn, rn;
+    xn.x = fmaf(alpha, p.x, x.x); xn.y = fmaf(alpha, p.y, x.y);
+    xn.z = fmaf(alpha, p.z, x.z); xn.w = fmaf(alpha, p.w, x.w);
+    rn.x = fmaf(-alpha, ap.x, r.x); rn.y = fmaf(-alpha, ap.y, r.y);
+    rn.z = fmaf(-alpha, ap.z, r.z); rn.w = fmaf(-alpha, ap.w, r.w);
+    st4v(U, o, xn);
+    st4v(G.r, o, rn);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        if (j + c < W) {
+            const float v = f4at(rn, c);
+            acc[0] += (double)v * (double)v;
+            acc[1] += isfinite(f4at(xn, c)) ? 0.0 : 1.0;
+        }
+    }
+    return rn;
+}
+
 template <int M, int MODE>
 __global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowf_bl(const GridDev* __restrict__ grids,
                                                                              const int* __restrict__ starts, int n,
@@ -37,10 +74,20 @@ __global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowf_bl(con
         const int i0 = 2 * pair, i1 = i0 + 1;
         const bool has1 = i1 < H;
         __syncthreads();  // previous row pair's reads of sm are done
-        for (int j = t; j < W; j += T) {
-            const float a = rowfwd_value<MODE>(G, U, pk, alpha, i0, j, acc);
-            const float b = has1 ? rowfwd_value<MODE>(G, U, pk, alpha, i1, j, acc) : 0.f;
-            sm[pad16(mk_perm(j, W))] = make_float2(a, b);
+        if (MODE == 2) {
+            for (int j = 4 * t; j < W; j += 4 * T) {
+                const float4 a = upd4(G, U, pk, alpha, i0, j, W, acc);
+                const float4 b = has1 ? upd4(G, U, pk, alpha, i1, j, W, acc) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int c = 0; c < 4; c++)
+                    if (j + c < W) sm[pad16(mk_perm(j + c, W))] = make_float2(f4at(a, c), f4at(b, c));
+            }
+        } else {
+            for (int j = t; j < W; j += T) {
+                const float a = rowfwd_value<MODE>(G, U, pk, alpha, i0, j, acc);
+                const float b = has1 ? rowfwd_value<MODE>(G, U, pk, alpha, i1, j, acc) : 0.f;
+                sm[pad16(mk_perm(j, W))] = make_float2(a, b);
+            }
         }
         __syncthreads();
         blue_fft<M>(sm, t, W, G.prow);
@@ -99,10 +146,33 @@ __global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowi_bl(con
         }
         __syncthreads();
         blue_fft<M>(sm, t, W, G.prow);
-        for (int j = t; j < W; j += T) {
-            const float2 v = sm[pad16(mk_perm(j, W))];
-            rowinv_store<MODE>(G, i0, j, v.x, beta, acc);
-            if (has1) rowinv_store<MODE>(G, i1, j, -v.y, beta, acc);
+        if (MODE == 2) {
+            // p = z + beta p in float4 groups (columns >= W of a group are padding)
+            for (int j = 4 * t; j < W; j += 4 * T) {
+                float za[4], zb[4];
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const float2 v = j + c < W ? sm[pad16(mk_perm(j + c, W))] : make_float2(0.f, 0.f);
+                    za[c] = v.x;
+                    zb[c] = -v.y;
+                }
+                const size_t oa = (size_t)i0 * P + j;
+                const float4 pa = ld4v(G.p0, oa);
+                st4v(G.p0, oa, make_float4(fadd(fmul(pa.x, beta), za[0]), fadd(fmul(pa.y, beta), za[1]),
+                                           fadd(fmul(pa.z, beta), za[2]), fadd(fmul(pa.w, beta), za[3])));
+                if (has1) {
+                    const size_t ob = oa + P;
+                    const float4 pb = ld4v(G.p0, ob);
+                    st4v(G.p0, ob, make_float4(fadd(fmul(pb.x, beta), zb[0]), fadd(fmul(pb.y, beta), zb[1]),
+                                               fadd(fmul(pb.z, beta), zb[2]), fadd(fmul(pb.w, beta), zb[3])));
+                }
+            }
+        } else {
+            for (int j = t; j < W; j += T) {
+                const float2 v = sm[pad16(mk_perm(j, W))];
+                rowinv_store<MODE>(G, i0, j, v.x, beta, acc);
+                if (has1) rowinv_store<MODE>(G, i1, j, -v.y, beta, acc);
+            }
         }
     }
     if (MODE != 0) return;

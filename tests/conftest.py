@@ -28,7 +28,9 @@ def load_golden(name):
 
 
 def small_golden_names():
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("L_"))
+    """Unwrapper fixtures (L_* are the large ones, gs_* belong to the Goldstein filter)."""
+    return sorted(f[:-4] for f in os.listdir(GOLDEN)
+                  if f.endswith(".npz") and not f.startswith("L_") and not f.startswith("gs_"))
 
 
 @pytest.fixture
