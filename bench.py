@@ -322,6 +322,31 @@ def run_b200(args):
                 "timing": f"per-launch CUDA events on the solve stream over a separate timed pass of "
                           f"{prof_steps} step(s) ({t_prof * 1e3:.1f} ms/step with the events)"}
 
+    # column pass: bound by instruction issue, not memory -> also its issue-rate roofline
+    # (warp instructions per launch from the ncu capture in profiles/, peak = 4 issue slots
+    # per SM per cycle at the sampled SM clock)
+    if os.path.exists(tf):
+        inst = json.load(open(tf)).get("inst", {}).get("col")
+        if inst and fam["col"][1]:
+            col_s = fam["col"][0] / 1e3 / fam["col"][1]
+            sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+            peak_i = 148 * 4 * sm_mhz * 1e6 / 1e9
+            roofline["col_issue"] = {"bound": "issue", "kernel": "col", "unit": "Ginst/s (warp)",
+                                     "inst_per_launch": inst, "achieved": round(inst / col_s / 1e9, 1),
+                                     "peak": round(peak_i, 1), "frac": round(inst / col_s / 1e9 / peak_i, 4)}
+
+    # ---- the 64-grid uneven stack (the other workload of the headline metric), sharded by grid
+    stack = None
+    if not args.no_stack_line:
+        _, sph, swt, s_npx = stack_grids(64, rank, world)
+        s_val, s_t, s_iters = stack_measure(sph, swt, 3, 2, world, local, s_npx)
+        stack = {"value": round(s_val, 3), "unit": UNIT, "ms_per_step": round(s_t * 1e3, 1), "steps": 2,
+                 "warmup": 3, "grids": 64, "total_mpx": round(s_npx / 1e6, 1),
+                 "workload": "64 G1 grids, rows U[1500,2600] x cols U[4000,7000], noise U[0.2,0.8], "
+                             "function defaults, one batched solve per step, inputs resident in HBM",
+                 "parallelism": f"grids sharded over {world} GPU(s)"}
+        del sph, swt
+
     # ---- CPU baseline (rank 0, N=1 only): the oracle on a bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -343,7 +368,8 @@ def run_b200(args):
                       "parallelism": f"replicas x{world}"},
            "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(npx * 8),
                    "d2h_bytes_per_step": int(npx * 6)},
-           "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches // 1}
+           "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches // 1,
+           "stack": stack}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
@@ -359,75 +385,89 @@ def _gen_stack_entry(m):
     return p, c
 
 
-def make_stack(n, workers=None):
-    """The uneven SBAS stack (rows U{1500..2600}, cols U{4000..7000}, noise U[0.2,0.8]),
-    generated in a spawned process pool before any GPU work."""
+def stack_grids(n, rank, world):
+    """This rank's share of the n-grid stack (grid indices, phases, weights), generated
+    in a spawned process pool (safe after CUDA is initialised); shapes come from the
+    seeded metadata, so every rank computes the same shard without communicating."""
     import multiprocessing as mproc
+    from core_b200.stack import shard_stack
     from oracle.generators import gen_stack_meta
     meta = gen_stack_meta(n, seed=0)
-    with mproc.get_context("spawn").Pool(workers or min(16, os.cpu_count() or 1)) as pool:
-        grids = pool.map(_gen_stack_entry, meta)
-    return [g[0] for g in grids], [g[1] for g in grids]
+    shapes = [(m[0], m[1]) for m in meta]
+    mine = shard_stack(shapes, world)[rank]
+    with mproc.get_context("spawn").Pool(min(16, os.cpu_count() or 1, max(1, len(mine)))) as pool:
+        grids = pool.map(_gen_stack_entry, [meta[i] for i in mine])
+    return mine, [g[0] for g in grids], [g[1] for g in grids], sum(h * w for h, w in shapes)
 
 
-def run_stack(args, phases, weights):
-    """K batched solves of this rank's share of the stack, inputs resident in HBM."""
+def stack_measure(phases, weights, warmup, steps, world, local, npx_all):
+    """Batched solves of this rank's grids, inputs resident in HBM: (Mpx/s over the whole
+    stack, seconds per step (max over ranks), per-grid IRLS counts)."""
     import torch
 
     from core_b200 import _lib
-    from core_b200.stack import shard_stack
     from core_b200.unwrap2d import make_params
 
-    rank, world, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
     lib = _lib.load()
-    mine = shard_stack([p.shape for p in phases], world)[rank]
-    n = len(mine)
-    grids = (_lib.UnwGrid * n)()
+    n = len(phases)
+    grids = (_lib.UnwGrid * max(n, 1))()
     keep = []
-    Hs, Ws = (C.c_int64 * n)(), (C.c_int64 * n)()
-    for k, i in enumerate(mine):
-        H, W = phases[i].shape
-        ph = torch.from_numpy(phases[i]).to(dev)
-        wt = torch.from_numpy(weights[i]).to(dev)
+    Hs, Ws = (C.c_int64 * max(n, 1))(), (C.c_int64 * max(n, 1))()
+    for k in range(n):
+        H, W = phases[k].shape
+        ph = torch.from_numpy(phases[k]).to(dev)
+        wt = torch.from_numpy(weights[k]).to(dev)
         ou = torch.empty((H, W), dtype=torch.float32, device=dev)
         oc = torch.empty((H, W), dtype=torch.int16, device=dev)
         keep += [ph, wt, ou, oc]
         grids[k] = _lib.UnwGrid(ph.data_ptr(), W, wt.data_ptr(), W, H, W, ou.data_ptr(), W, oc.data_ptr(), W)
         Hs[k], Ws[k] = H, W
-    ws = torch.empty(lib.unw_batch_workspace_bytes(n, Hs, Ws), dtype=torch.uint8, device=dev)
+    ws = torch.empty(lib.unw_batch_workspace_bytes(n, Hs, Ws) if n else 1, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
-    sts = (_lib.UnwStats * n)()
+    sts = (_lib.UnwStats * max(n, 1))()
     prm = make_params(**FN)
 
     def solve():
-        _lib.check(lib.unw_solve_batch(n, grids, C.byref(prm), ws.data_ptr(), ws.numel(), sts, stream.cuda_stream))
+        if n:
+            _lib.check(lib.unw_solve_batch(n, grids, C.byref(prm), ws.data_ptr(), ws.numel(), sts,
+                                           stream.cuda_stream))
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         solve()
-    clocks = ClockSampler(local)
-    clocks.start()
     barrier(world)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         solve()
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
-    clk = clocks.stop()
     t = barrier_max(ev0.elapsed_time(ev1) / 1e3, world, local)
-    npx_all = sum(p.size for p in phases)
-    value = npx_all * args.steps / 1e6 / t
+    iters = [sts[k].irls_iters for k in range(n)]
+    del keep, ws
+    torch.cuda.empty_cache()
+    return npx_all * steps / 1e6 / t, t / steps, iters
+
+
+def run_stack(args):
+    """K batched solves of this rank's share of the stack, inputs resident in HBM."""
+    import torch
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(torch.device("cuda", local))
+    mine, phases, weights, npx_all = stack_grids(args.stack, rank, world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    value, t_step, iters = stack_measure(phases, weights, args.warmup, args.steps, world, local, npx_all)
+    clk = clocks.stop()
     out = {"metric": "unwrapped Mpx/s (64-interferogram uneven stack, function-default iterations)",
            "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": round(t / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "strong",
+           "ms_per_step": round(t_step * 1e3, 3), "higher_is_better": True, "scaling": "strong",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": f"stack of {len(phases)} G1 grids, rows U[1500,2600] x cols U[4000,7000]",
-                      "total_mpx": round(npx_all / 1e6, 1), "params": FN,
-                      "irls_iters": [sts[k].irls_iters for k in range(n)],
+           "config": {"workload": f"stack of {args.stack} G1 grids, rows U[1500,2600] x cols U[4000,7000]",
+                      "total_mpx": round(npx_all / 1e6, 1), "params": FN, "irls_iters_rank0": iters,
                       "l2": "working set tens of GB, far above the 126 MB L2",
                       "parallelism": f"grids sharded over {world} GPU(s)"},
            "clocks": clk}
@@ -448,12 +488,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--stack", type=int, default=0,
                     help="measure the uneven SBAS stack of this many grids instead of the 4096^2 grid")
+    ap.add_argument("--no-stack-line", action="store_true",
+                    help="leave the 64-grid stack sub-measurement out of the default line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.stack:
-        phases, weights = make_stack(args.stack)
-        return run_stack(args, phases, weights)
+        return run_stack(args)
     return run_b200(args)
 
 
