@@ -78,13 +78,17 @@ long long next_pow2(long long x) {
     while (p < x) p <<= 1;
     return p;
 }
-// Bluestein length M (power of two >= 2N - 1, >= 256) of the register-FFT path
-// for a DCT length N that is not a power of two; 0 where that path is not used
-// (powers of two have their own kernels; very short axes stay on the generic
+// Bluestein length M >= 2N - 1 of the register-FFT path for a DCT length N that
+// is not a power of two: the shorter of the power of two (>= 256) and three
+// times a power of two (>= 768) that fit; 0 where the path is not used (powers
+// of two have their own kernels; very short axes stay on the generic
 // shared-memory FFT; N > 8192 would need M > 16384).
 int bl_len(int N) {
     if (N <= 64 || 2LL * N - 1 > MAX_FFT || (N & (N - 1)) == 0) return 0;
-    return (int)std::max<long long>(256, next_pow2(2LL * N - 1));
+    const long long need = 2LL * N - 1;
+    const long long m2 = std::max<long long>(256, next_pow2(need));
+    const long long m3 = 3 * std::max<long long>(256, next_pow2((need + 2) / 3));
+    return (int)std::min(m2, m3);
 }
 
 std::vector<int> factor(int n) {

@@ -2,7 +2,7 @@
 // on T) for column lengths N that are not powers of two (64 < N <= 8192):
 // NSEQ column pairs per CTA, each pair one complex sequence handled by M / 16
 // threads, the length-N DFTs by Bluestein on the register FFT of length
-// M = the power of two >= 2N - 1 (unw_bluestein.cuh).  MODE 0: DCT initial
+// M >= 2N - 1, a power of two or three times one (unw_bluestein.cuh).  MODE 0: DCT initial
 // solve; MODE 1 / 2: PCG (gated), with r.z by Parseval (col_spectral_pair)
 // and its scalar step (col_finalize).
 #include "unw_bluestein.cuh"
@@ -14,13 +14,13 @@ namespace {
 template <int T>
 constexpr int bl_min_blocks() { return T >= 1024 ? 1 : (1024 / T > 16 ? 16 : 1024 / T); }
 
-template <int M>
-constexpr int bl_col_nseq() { return M >= 8192 ? 1 : (8192 / M > 8 ? 8 : 8192 / M); }
+// column pairs per CTA: about 512 threads per CTA, at most 8 pairs
+constexpr int bl_col_nseq_len(int M) { return M >= 8192 ? 1 : (8192 / M > 8 ? 8 : (8192 / M < 1 ? 1 : 8192 / M)); }
 
-template <int M, int NSEQ, int MODE>
-__global__ void __launch_bounds__(M / 16 * NSEQ, bl_min_blocks<M / 16 * NSEQ>()) k_col_bl(
+template <class BL, int NSEQ, int MODE>
+__global__ void __launch_bounds__(BL::T * NSEQ, bl_min_blocks<BL::T * NSEQ>()) k_col_bl(
     const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
-    constexpr int T = M / 16;
+    constexpr int T = BL::T;
     extern __shared__ float2 sm[];
     __shared__ double red[32];
     const int g = find_grid(starts, n, blockIdx.x);
@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(M / 16 * NSEQ, bl_min_blocks<M / 16 * NSEQ>())
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
     const int s = threadIdx.x % NSEQ, t = threadIdx.x / NSEQ;
-    float2* sms = sm + s * RegFft<M>::SEQ_STRIDE;
+    float2* sms = sm + s * BL::SLOTS;
     float* __restrict__ Tm = G.T;
     const float2* __restrict__ dw = G.pcol.dctw;
     const float* __restrict__ sH = G.sH;
@@ -48,26 +48,26 @@ __global__ void __launch_bounds__(M / 16 * NSEQ, bl_min_blocks<M / 16 * NSEQ>())
             float2 x = make_float2(0.f, 0.f);
             if (hasb) x = make_float2(a[0], a[1]);
             else if (hasa) x.x = a[0];
-            sms[pad16(mk_perm(i, H))] = x;
+            sms[BL::pos(mk_perm(i, H))] = x;
         }
         __syncthreads();
-        blue_fft<M>(sms, t, H, G.pcol);
+        BL::dft(sms, t, H, G.pcol);
         const float ca = hasa ? G.sW[ja] : 1.0f, cb = hasb ? G.sW[ja + 1] : 1.0f;
         for (int k = t; k <= H / 2; k += T) {
             const int km = k == 0 ? 0 : H - k;
-            const float2 C = sms[pad16(k)], Cm = sms[pad16(km)];
+            const float2 C = sms[BL::pos(k)], Cm = sms[BL::pos(km)];
             const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
             const float ck = __ldg(&sH[k]), cm = __ldg(&sH[km]);
             float2 ok, om;
             col_spectral_pair<(MODE >= 1)>(C, Cm, k, km, wk, wm, ck, cm, ca, cb, ja == 0, hasb, negs, ok, om,
                                            acc[0]);
-            if (km != k) sms[pad16(km)] = om;
-            sms[pad16(k)] = ok;
+            if (km != k) sms[BL::pos(km)] = om;
+            sms[BL::pos(k)] = ok;
         }
         __syncthreads();
-        blue_fft<M>(sms, t, H, G.pcol);
+        BL::dft(sms, t, H, G.pcol);
         for (int i = t; i < H; i += T) {
-            const float2 v = sms[pad16(mk_perm(i, H))];
+            const float2 v = sms[BL::pos(mk_perm(i, H))];
             float* a = Tm + (size_t)i * P + ja;
             if (hasb) { a[0] = v.x; a[1] = -v.y; }
             else if (hasa) a[0] = v.x;
@@ -80,19 +80,19 @@ __global__ void __launch_bounds__(M / 16 * NSEQ, bl_min_blocks<M / 16 * NSEQ>())
     }
 }
 
-template <int M>
+template <class BL>
 cudaError_t col_bl_m(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* st, int n) {
-    constexpr int NS = bl_col_nseq<M>();
-    const size_t smem = sizeof(float2) * (size_t)RegFft<M>::SEQ_STRIDE * NS;
+    constexpr int NS = bl_col_nseq_len(BL::LEN);
+    const size_t smem = sizeof(float2) * (size_t)BL::SLOTS * NS;
     auto go = [&](auto kfn) {
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kfn<<<nblk, M / 16 * NS, smem, s>>>(gd, st, n);
+        kfn<<<nblk, BL::T * NS, smem, s>>>(gd, st, n);
         return cudaGetLastError();
     };
     switch (mode) {
-        case 0: return go(k_col_bl<M, NS, 0>);
-        case 1: return go(k_col_bl<M, NS, 1>);
-        default: return go(k_col_bl<M, NS, 2>);
+        case 0: return go(k_col_bl<BL, NS, 0>);
+        case 1: return go(k_col_bl<BL, NS, 1>);
+        default: return go(k_col_bl<BL, NS, 2>);
     }
 }
 
@@ -100,13 +100,8 @@ cudaError_t col_bl_m(int mode, int nblk, cudaStream_t s, const GridDev* gd, cons
 
 int unw_bl_col_nseq(int M) {
     switch (M) {
-        case 256: return bl_col_nseq<256>();
-        case 512: return bl_col_nseq<512>();
-        case 1024: return bl_col_nseq<1024>();
-        case 2048: return bl_col_nseq<2048>();
-        case 4096: return bl_col_nseq<4096>();
-        case 8192: return bl_col_nseq<8192>();
-        case 16384: return bl_col_nseq<16384>();
+        case 256: case 512: case 1024: case 2048: case 4096: case 8192: case 16384:
+        case 768: case 1536: case 3072: case 6144: case 12288: return bl_col_nseq_len(M);
         default: return 0;
     }
 }
@@ -115,13 +110,18 @@ cudaError_t unw_launch_col_bl(int M, int mode, int nblk, cudaStream_t s, const G
                               int n) {
     if (nblk <= 0) return cudaSuccess;
     switch (M) {
-        case 256: return col_bl_m<256>(mode, nblk, s, gd, starts, n);
-        case 512: return col_bl_m<512>(mode, nblk, s, gd, starts, n);
-        case 1024: return col_bl_m<1024>(mode, nblk, s, gd, starts, n);
-        case 2048: return col_bl_m<2048>(mode, nblk, s, gd, starts, n);
-        case 4096: return col_bl_m<4096>(mode, nblk, s, gd, starts, n);
-        case 8192: return col_bl_m<8192>(mode, nblk, s, gd, starts, n);
-        case 16384: return col_bl_m<16384>(mode, nblk, s, gd, starts, n);
+        case 256: return col_bl_m<BlP2<256>>(mode, nblk, s, gd, starts, n);
+        case 512: return col_bl_m<BlP2<512>>(mode, nblk, s, gd, starts, n);
+        case 1024: return col_bl_m<BlP2<1024>>(mode, nblk, s, gd, starts, n);
+        case 2048: return col_bl_m<BlP2<2048>>(mode, nblk, s, gd, starts, n);
+        case 4096: return col_bl_m<BlP2<4096>>(mode, nblk, s, gd, starts, n);
+        case 8192: return col_bl_m<BlP2<8192>>(mode, nblk, s, gd, starts, n);
+        case 16384: return col_bl_m<BlP2<16384>>(mode, nblk, s, gd, starts, n);
+        case 768: return col_bl_m<BlMix3<256>>(mode, nblk, s, gd, starts, n);
+        case 1536: return col_bl_m<BlMix3<512>>(mode, nblk, s, gd, starts, n);
+        case 3072: return col_bl_m<BlMix3<1024>>(mode, nblk, s, gd, starts, n);
+        case 6144: return col_bl_m<BlMix3<2048>>(mode, nblk, s, gd, starts, n);
+        case 12288: return col_bl_m<BlMix3<4096>>(mode, nblk, s, gd, starts, n);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -2,8 +2,8 @@
 // the same row-pair structure as the power-of-two kernels (two real rows are
 // one complex sequence, Makhoul's reordering is a scatter/gather through
 // shared memory), with the length-N DFT done by Bluestein on the register FFT
-// of length M = the power of two >= 2N - 1 (unw_bluestein.cuh).  M / 16
-// threads per CTA; the CTA loops over row pairs.
+// of length M >= 2N - 1, a power of two or three times one (unw_bluestein.cuh).
+// M / 16 threads per CTA; the CTA loops over row pairs.
 #include "unw_bluestein.cuh"
 #include "unw_rowops.cuh"
 #include "unw_kernels.h"
@@ -50,11 +50,11 @@ __device__ __forceinline__ float4 upd4(const GridDev& G, float* __restrict__ U, 
     return rn;
 }
 
-template <int M, int MODE>
-__global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowf_bl(const GridDev* __restrict__ grids,
-                                                                             const int* __restrict__ starts, int n,
-                                                                             int it, int cgk) {
-    constexpr int T = M / 16;
+template <class BL, int MODE>
+__global__ void __launch_bounds__(BL::T, bl_min_blocks<BL::T>()) k_rowf_bl(const GridDev* __restrict__ grids,
+                                                                           const int* __restrict__ starts, int n,
+                                                                           int it, int cgk) {
+    constexpr int T = BL::T;
     extern __shared__ float2 sm[];
     __shared__ double red[32 * 2];
     const int g = find_grid(starts, n, blockIdx.x);
@@ -80,23 +80,23 @@ __global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowf_bl(con
                 const float4 b = has1 ? upd4(G, U, pk, alpha, i1, j, W, acc) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
                 for (int c = 0; c < 4; c++)
-                    if (j + c < W) sm[pad16(mk_perm(j + c, W))] = make_float2(f4at(a, c), f4at(b, c));
+                    if (j + c < W) sm[BL::pos(mk_perm(j + c, W))] = make_float2(f4at(a, c), f4at(b, c));
             }
         } else {
             for (int j = t; j < W; j += T) {
                 const float a = rowfwd_value<MODE>(G, U, pk, alpha, i0, j, acc);
                 const float b = has1 ? rowfwd_value<MODE>(G, U, pk, alpha, i1, j, acc) : 0.f;
-                sm[pad16(mk_perm(j, W))] = make_float2(a, b);
+                sm[BL::pos(mk_perm(j, W))] = make_float2(a, b);
             }
         }
         __syncthreads();
-        blue_fft<M>(sm, t, W, G.prow);
+        BL::dft(sm, t, W, G.prow);
         // two real rows from one complex DFT, then X_k = Re(exp(-i pi k/2W) V_k)
         float* __restrict__ Ta = G.T + (size_t)i0 * P;
         float* __restrict__ Tb = G.T + (size_t)i1 * P;
         for (int k = t; k < W; k += T) {
-            const float2 C = sm[pad16(k)];
-            const float2 Cm = sm[pad16(k == 0 ? 0 : W - k)];
+            const float2 C = sm[BL::pos(k)];
+            const float2 Cm = sm[BL::pos(k == 0 ? 0 : W - k)];
             const float2 w = __ldg(&dw[k]);
             const float2 Va = make_float2(C.x + Cm.x, C.y - Cm.y);
             const float2 Vb = make_float2(C.y + Cm.y, Cm.x - C.x);
@@ -111,10 +111,10 @@ __global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowf_bl(con
     }
 }
 
-template <int M, int MODE>
-__global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowi_bl(const GridDev* __restrict__ grids,
-                                                                             const int* __restrict__ starts, int n) {
-    constexpr int T = M / 16;
+template <class BL, int MODE>
+__global__ void __launch_bounds__(BL::T, bl_min_blocks<BL::T>()) k_rowi_bl(const GridDev* __restrict__ grids,
+                                                                           const int* __restrict__ starts, int n) {
+    constexpr int T = BL::T;
     extern __shared__ float2 sm[];
     __shared__ double red[32 * 2];
     const int g = find_grid(starts, n, blockIdx.x);
@@ -142,17 +142,17 @@ __global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowi_bl(con
             const float2 wc = cconj(__ldg(&dw[k]));
             const float2 Pa = cmul(wc, make_float2(ya, -yam));
             const float2 Pb = cmul(wc, make_float2(yb, -ybm));
-            sm[pad16(k)] = cconj(make_float2(Pa.x - Pb.y, Pa.y + Pb.x));
+            sm[BL::pos(k)] = cconj(make_float2(Pa.x - Pb.y, Pa.y + Pb.x));
         }
         __syncthreads();
-        blue_fft<M>(sm, t, W, G.prow);
+        BL::dft(sm, t, W, G.prow);
         if (MODE == 2) {
             // p = z + beta p in float4 groups (columns >= W of a group are padding)
             for (int j = 4 * t; j < W; j += 4 * T) {
                 float za[4], zb[4];
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
-                    const float2 v = j + c < W ? sm[pad16(mk_perm(j + c, W))] : make_float2(0.f, 0.f);
+                    const float2 v = j + c < W ? sm[BL::pos(mk_perm(j + c, W))] : make_float2(0.f, 0.f);
                     za[c] = v.x;
                     zb[c] = -v.y;
                 }
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowi_bl(con
             }
         } else {
             for (int j = t; j < W; j += T) {
-                const float2 v = sm[pad16(mk_perm(j, W))];
+                const float2 v = sm[BL::pos(mk_perm(j, W))];
                 rowinv_store<MODE>(G, i0, j, v.x, beta, acc);
                 if (has1) rowinv_store<MODE>(G, i1, j, -v.y, beta, acc);
             }
@@ -182,56 +182,62 @@ __global__ void __launch_bounds__(M / 16, bl_min_blocks<M / 16>()) k_rowi_bl(con
     }
 }
 
-template <int M>
+template <class BL>
 cudaError_t rowf_bl_m(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* st, int n, int it, int cgk) {
-    const size_t smem = sizeof(float2) * RegFft<M>::SMEM;
+    const size_t smem = sizeof(float2) * BL::SLOTS;
     auto go = [&](auto kfn) {
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kfn<<<nblk, M / 16, smem, s>>>(gd, st, n, it, cgk);
+        kfn<<<nblk, BL::T, smem, s>>>(gd, st, n, it, cgk);
         return cudaGetLastError();
     };
     switch (mode) {
-        case 0: return go(k_rowf_bl<M, 0>);
-        case 1: return go(k_rowf_bl<M, 1>);
-        case 2: return go(k_rowf_bl<M, 2>);
-        default: return go(k_rowf_bl<M, 3>);
+        case 0: return go(k_rowf_bl<BL, 0>);
+        case 1: return go(k_rowf_bl<BL, 1>);
+        case 2: return go(k_rowf_bl<BL, 2>);
+        default: return go(k_rowf_bl<BL, 3>);
     }
 }
 
-template <int M>
+template <class BL>
 cudaError_t rowi_bl_m(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* st, int n) {
-    const size_t smem = sizeof(float2) * RegFft<M>::SMEM;
+    const size_t smem = sizeof(float2) * BL::SLOTS;
     auto go = [&](auto kfn) {
         cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kfn<<<nblk, M / 16, smem, s>>>(gd, st, n);
+        kfn<<<nblk, BL::T, smem, s>>>(gd, st, n);
         return cudaGetLastError();
     };
     switch (mode) {
-        case 0: return go(k_rowi_bl<M, 0>);
-        case 1: return go(k_rowi_bl<M, 1>);
-        case 2: return go(k_rowi_bl<M, 2>);
-        default: return go(k_rowi_bl<M, 3>);
+        case 0: return go(k_rowi_bl<BL, 0>);
+        case 1: return go(k_rowi_bl<BL, 1>);
+        case 2: return go(k_rowi_bl<BL, 2>);
+        default: return go(k_rowi_bl<BL, 3>);
     }
 }
 
 }  // namespace
 
-#define UNW_BL_SWITCH(M, CALL)                 \
-    switch (M) {                               \
-        case 256: return CALL(256);            \
-        case 512: return CALL(512);            \
-        case 1024: return CALL(1024);          \
-        case 2048: return CALL(2048);          \
-        case 4096: return CALL(4096);          \
-        case 8192: return CALL(8192);          \
-        case 16384: return CALL(16384);        \
-        default: return cudaErrorInvalidValue; \
+// Bluestein lengths: powers of two 256..16384 and three times powers of two 768..12288
+#define UNW_BL_SWITCH(M, CALL)                    \
+    switch (M) {                                  \
+        case 256: return CALL(BlP2<256>);         \
+        case 512: return CALL(BlP2<512>);         \
+        case 1024: return CALL(BlP2<1024>);       \
+        case 2048: return CALL(BlP2<2048>);       \
+        case 4096: return CALL(BlP2<4096>);       \
+        case 8192: return CALL(BlP2<8192>);       \
+        case 16384: return CALL(BlP2<16384>);     \
+        case 768: return CALL(BlMix3<256>);       \
+        case 1536: return CALL(BlMix3<512>);      \
+        case 3072: return CALL(BlMix3<1024>);     \
+        case 6144: return CALL(BlMix3<2048>);     \
+        case 12288: return CALL(BlMix3<4096>);    \
+        default: return cudaErrorInvalidValue;    \
     }
 
 cudaError_t unw_launch_rowf_bl(int M, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
                                int n, int it, int cgk) {
     if (nblk <= 0) return cudaSuccess;
-#define CALL(MM) rowf_bl_m<MM>(mode, nblk, s, gd, starts, n, it, cgk)
+#define CALL(BB) rowf_bl_m<BB>(mode, nblk, s, gd, starts, n, it, cgk)
     UNW_BL_SWITCH(M, CALL)
 #undef CALL
 }
@@ -239,7 +245,7 @@ cudaError_t unw_launch_rowf_bl(int M, int mode, int nblk, cudaStream_t s, const 
 cudaError_t unw_launch_rowi_bl(int M, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
                                int n) {
     if (nblk <= 0) return cudaSuccess;
-#define CALL(MM) rowi_bl_m<MM>(mode, nblk, s, gd, starts, n)
+#define CALL(BB) rowi_bl_m<BB>(mode, nblk, s, gd, starts, n)
     UNW_BL_SWITCH(M, CALL)
 #undef CALL
 }

@@ -56,8 +56,9 @@ __device__ __forceinline__ void twiddle_row(float2* w, float2 w1) {
 
 // One Stockham pass of radix R with NS = product of earlier radices.
 // Butterfly j = t + b*T (b < 16/R) reads elements j + r*(N/R) and writes
-// (j - k)*R + k + r*NS, k = j mod NS.
-template <int N, int R, int NS, bool FIRST, bool LAST>
+// (j - k)*R + k + r*NS, k = j mod NS.  The twiddle table holds exp(-2 pi i m / (N*TS)):
+// TS > 1 lets a length-N transform use the table of a TS times longer one.
+template <int N, int R, int NS, bool FIRST, bool LAST, int TS = 1>
 __device__ __forceinline__ void reg_pass(float2 (&v)[16], float2* __restrict__ sm, int t,
                                          const float2* __restrict__ tw) {
     constexpr int T = N / 16;
@@ -81,7 +82,7 @@ __device__ __forceinline__ void reg_pass(float2 (&v)[16], float2* __restrict__ s
     for (int b = 0; b < NB; b++) {
         const int j = t + b * T;
         const int k = j & (NS - 1);
-        if (NS > 1) twiddle_row<R>(w[b], __ldg(&tw[k * S]));
+        if (NS > 1) twiddle_row<R>(w[b], __ldg(&tw[k * S * TS]));
         Dft<R>::run(w[b]);
         if (LAST) {
 #pragma unroll
@@ -112,13 +113,13 @@ __device__ __forceinline__ void reg_fft_rec(float2 (&v)[16], float2* sm, int t, 
     }
 }
 
-template <int N, int P, int NS>
+template <int N, int P, int NS, int TS = 1>
 __device__ __forceinline__ void smem_fft_rec(float2* sm, int t, const float2* tw) {
     if constexpr (P < RegFft<N>::NPASS) {
         constexpr int R = (P < RegFft<N>::NP16) ? 16 : (1 << RegFft<N>::REM);
         float2 v[16];
-        reg_pass<N, R, NS, false, false>(v, sm, t, tw);
-        smem_fft_rec<N, P + 1, NS * R>(sm, t, tw);
+        reg_pass<N, R, NS, false, false, TS>(v, sm, t, tw);
+        smem_fft_rec<N, P + 1, NS * R, TS>(sm, t, tw);
     }
 }
 
@@ -142,9 +143,9 @@ __device__ __forceinline__ void io_fft(float2 (&v)[16], float2* sm, int t, const
 // addresses pad16(i)), result in place.  Registers are used only inside each
 // pass.  The caller synchronises before the call (inputs written) and the
 // result is visible to all threads on return.
-template <int N>
+template <int N, int TS = 1>
 __device__ __forceinline__ void smem_fft(float2* sm, int t, const float2* tw) {
-    smem_fft_rec<N, 0, 1>(sm, t, tw);
+    smem_fft_rec<N, 0, 1, TS>(sm, t, tw);
 }
 
 // Forward FFT (exp(-2 pi i nk/N)) in place in the stride-T register layout.

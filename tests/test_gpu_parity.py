@@ -139,7 +139,10 @@ def ref_setup(phase, weight):
 # ------------------------------------------------------------------ operator kernels
 SHAPES = [(64, 64), (37, 50), (128, 96), (17, 257), (1, 7), (5, 1), (3, 5), (1, 1), (200, 131),
           (1024, 1024), (2600, 4001), (4096, 4096), (256, 512), (512, 256), (2048, 1000), (1000, 2048),
-          (4096, 333), (6, 16384), (8192, 10)]
+          (4096, 333), (6, 16384), (8192, 10),
+          # Bluestein lengths three times a power of two: 768 (N=300), 1536 (700), 3072 (1400),
+          # 6144 (2500), 12288 (5000); and 8191 (M = 16384)
+          (700, 300), (1400, 96), (96, 2500), (300, 5000), (2500, 700), (70, 8191)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
