@@ -12,7 +12,9 @@
 // x_m in sm[pad16(m)], m < N (written and synchronised by the caller) ->
 // X_k in sm[pad16(k)], k < N, synchronised on return.  M / 16 threads per
 // sequence, t = this thread's index within its sequence; every thread of the
-// CTA must call (the FFT passes synchronise the CTA).
+// CTA must call (the FFT passes synchronise the CTA).  The data stays in shared
+// memory between the steps (measured faster than carrying it in registers
+// across the two FFTs, which spills at these thread counts).
 template <int M>
 __device__ __forceinline__ void blue_fft(float2* __restrict__ sm, int t, int N, const DctPlanDev& P) {
     constexpr int T = M / 16;
@@ -23,12 +25,13 @@ __device__ __forceinline__ void blue_fft(float2* __restrict__ sm, int t, int N, 
         sm[a] = m < N ? cmul(sm[a], cconj(__ldg(&ch[m]))) : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    float2 v[16];
-    io_fft<M, false, true>(v, sm, t, P.fft.tw);
-#pragma unroll
-    for (int q = 0; q < 16; q++) v[q] = cconj(cmul(v[q], __ldg(&hs[t + T * q])));
-    // the last pass above synchronised after its reads: sm may be overwritten
-    io_fft<M, true, false>(v, sm, t, P.fft.tw);
+    smem_fft<M>(sm, t, P.fft.tw);
+    for (int m = t; m < M; m += T) {
+        const int a = pad16(m);
+        sm[a] = cconj(cmul(sm[a], __ldg(&hs[m])));
+    }
+    __syncthreads();
+    smem_fft<M>(sm, t, P.fft.tw);
     for (int k = t; k < N; k += T) {
         const int a = pad16(k);
         sm[a] = cmul(cconj(sm[a]), cconj(__ldg(&ch[k])));
