@@ -142,10 +142,19 @@ def barrier(world):
         dist.barrier()
 
 
-def make_input(seed=0):
+def make_input(seed=0, shape=None):
+    """The 4096^2 G2 fault grid, or a G1 grid of the given (H, W) (seed + 1)."""
+    if shape:
+        from oracle.generators import gen_g1
+        p, c, _ = gen_g1(int(shape[0]), int(shape[1]), seed=seed + 1)
+        return p, c
     from oracle.generators import gen_g2
     p, c, _ = gen_g2(4096, seed=seed)
     return p, c
+
+
+def workload_name(shape):
+    return f"g1_{shape[0]}x{shape[1]} fn-defaults" if shape else "g2_4096 fn-defaults"
 
 
 # --------------------------------------------------------------------------- CPU baseline
@@ -172,7 +181,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     workers = os.cpu_count()
-    p, c = make_input()
+    p, c = make_input(shape=args.shape)
     npx = p.size
     n_irls = 30  # IRLS iterations of this solve under function defaults (reference CPU run)
     from oracle.irls_oracle import irls_unwrap_2d as oracle
@@ -194,7 +203,7 @@ def run_reference(args):
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": full * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-           "config": {"workload": "g2_4096 fn-defaults", "grid": [4096, 4096], "params": FN},
+           "config": {"workload": workload_name(args.shape), "grid": list(p.shape), "params": FN},
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -213,7 +222,7 @@ def run_b200(args):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     lib = _lib.load()
-    p, c = make_input(seed=rank)
+    p, c = make_input(seed=rank, shape=args.shape)
     H, W = p.shape
     npx = H * W
 
@@ -361,7 +370,7 @@ def run_b200(args):
     out = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(t_dev / args.steps * 1e3, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": "g2_4096 fn-defaults (one full unwrap per step, replica per GPU)",
+           "config": {"workload": workload_name(args.shape) + " (one full unwrap per step, replica per GPU)",
                       "grid": [H, W], "params": FN, "irls_iters": stats["irls_iters"],
                       "pcg_iters": stats["cg_iters_total"],
                       "l2": "inputs 134 MB and solver working set ~1.1 GB exceed the 126 MB L2",
@@ -488,6 +497,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--stack", type=int, default=0,
                     help="measure the uneven SBAS stack of this many grids instead of the 4096^2 grid")
+    ap.add_argument("--shape", type=int, nargs=2, default=None, metavar=("H", "W"),
+                    help="time a G1 grid of this shape instead of the 4096^2 fault grid")
     ap.add_argument("--no-stack-line", action="store_true",
                     help="leave the 64-grid stack sub-measurement out of the default line")
     args = ap.parse_args()
