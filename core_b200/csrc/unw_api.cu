@@ -53,7 +53,10 @@ constexpr size_t ALIGN = 256;
 constexpr int HIST_CAP = 65536;
 constexpr int ELEM_MAX_CTAS = 1184;      // 8 x 148 SMs
 constexpr size_t COL_SMEM_BUDGET = 96 * 1024;
-constexpr int MAX_FFT = 16384;           // longest transform one CTA holds (1024 threads x 16)
+constexpr int MAX_FFT = 16384;           // longest register FFT (1024 threads x 16)
+// longest transform of the shared-memory FFT (1024 threads x up to 32 elements,
+// one 8-byte slot per element within the 227 KB of shared memory a CTA can have)
+constexpr int MAX_GEN = 28672;
 // CTAs of the persistent PCG kernels (148 SMs x resident CTAs per SM)
 constexpr int NUM_SMS = 148;
 constexpr int CTAS_ROW = NUM_SMS * 4;
@@ -104,10 +107,13 @@ std::vector<int> factor(int n) {
     if (twos == 1) r.insert(r.begin(), 2);
     return r;
 }
+// elements per thread of the shared-memory FFT: 16, or 32 for lengths a
+// 1024-thread CTA cannot cover with 16
+int emax_of(long long n) { return n > 16384 ? 32 : EMAX; }
 // complex elements one thread can hold per pass, over the radices of a plan
-int plan_cap(const std::vector<int>& rad) {
-    int c = EMAX;
-    for (int R : rad) c = std::min(c, (EMAX / R) * R);
+int plan_cap(const std::vector<int>& rad, int emax) {
+    int c = emax;
+    for (int R : rad) c = std::min(c, (emax / R) * R);
     return c;
 }
 int pick_threads(long long elems, int cap) {
@@ -117,7 +123,7 @@ int pick_threads(long long elems, int cap) {
 }
 
 struct HostPlan {
-    int N = 0, n = 0, blue = 0, cap = 0;
+    int N = 0, n = 0, blue = 0, cap = 0, emax = 16;
     std::vector<int> rad;
 };
 HostPlan make_plan(int N) {
@@ -127,7 +133,8 @@ HostPlan make_plan(int N) {
     p.blue = (M || !smooth7(N)) ? 1 : 0;
     p.n = M ? M : fft_len(N);
     p.rad = p.n > 1 ? factor(p.n) : std::vector<int>{};
-    p.cap = plan_cap(p.rad);
+    p.emax = emax_of(p.n);
+    p.cap = plan_cap(p.rad, p.emax);
     return p;
 }
 
@@ -222,6 +229,7 @@ BatchLayout batch_layout(int n, const long long* H, const long long* W) {
 // ------------------------------------------------------------ launch shapes
 struct Shape {
     int row_T = 0, col_T = 0;
+    int row_emax = 16, col_emax = 16;   // elements per thread of the shared-memory FFT
     size_t row_smem = 0, col_smem = 0;
     int row_p2 = 0, col_p2 = 0;   // power-of-two register-FFT paths (length), 0 = generic
     int row_bl = 0, col_bl = 0;   // Bluestein register-FFT paths (FFT length M), 0 = not used
@@ -311,19 +319,20 @@ cudaError_t L_rowf(Solver& S, int mode, int it, int cgk) {
         return unw_launch_rowf_p2(S.sh.row_p2, mode, S.total[KS_ROWPAIR], S.s, S.dg, S.ds(KS_ROWPAIR), S.n, it, cgk);
     if (S.sh.row_bl)
         return unw_launch_rowf_bl(S.sh.row_bl, mode, S.total[KS_ROWPAIR], S.s, S.dg, S.ds(KS_ROWPAIR), S.n, it, cgk);
-    return unw_launch_row_fwd(mode, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg,
+    return unw_launch_row_fwd(mode, S.sh.row_T, S.sh.row_emax, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg,
                               S.ds(KS_ROWPAIR), S.n, it, cgk);
 }
 cudaError_t L_rowi(Solver& S, int mode) {
     if (S.sh.row_p2) return unw_launch_rowi_p2(S.sh.row_p2, mode, S.total[KS_ROWPAIR], S.s, S.dg, S.ds(KS_ROWPAIR), S.n);
     if (S.sh.row_bl) return unw_launch_rowi_bl(S.sh.row_bl, mode, S.total[KS_ROWPAIR], S.s, S.dg, S.ds(KS_ROWPAIR), S.n);
-    return unw_launch_row_inv(mode, S.sh.row_T, EMAX, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg,
+    return unw_launch_row_inv(mode, S.sh.row_T, S.sh.row_emax, S.total[KS_ROWPAIR], S.sh.row_smem, S.s, S.dg,
                               S.ds(KS_ROWPAIR), S.n);
 }
 cudaError_t L_col(Solver& S, int mode) {
     if (S.sh.col_p2) return unw_launch_col_p2(S.sh.col_p2, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n);
     if (S.sh.col_bl) return unw_launch_col_bl(S.sh.col_bl, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n);
-    return unw_launch_col(mode, S.sh.col_T, EMAX, S.total[KS_COL], S.sh.col_smem, S.s, S.dg, S.ds(KS_COL), S.n);
+    return unw_launch_col(mode, S.sh.col_T, S.sh.col_emax, S.total[KS_COL], S.sh.col_smem, S.s, S.dg, S.ds(KS_COL),
+                          S.n);
 }
 
 // ------------------------------------------------------------ IRLS enqueue
@@ -424,14 +433,14 @@ std::array<int, 4> group_key(int H, int W) {
     std::array<int, 4> k{};
     if (p2(W)) { k[0] = 1; k[1] = W; }
     else if (bl_len(W)) { k[0] = 2; k[1] = bl_len(W); }
-    else { const HostPlan hp = make_plan(W); k[0] = 0; k[1] = pick_threads(hp.n, hp.cap); }
+    else { const HostPlan hp = make_plan(W); k[0] = 0; k[1] = pick_threads(hp.n, hp.cap) * 64 + hp.emax; }
     if (p2(H)) { k[2] = 1; k[3] = H; }
     else if (bl_len(H)) { k[2] = 2; k[3] = bl_len(H); }
     else {
         const HostPlan hp = make_plan(H);
         int nseq = col_nseq_generic(hp.n, W), cT = 0;
         while (nseq >= 1 && !(cT = pick_threads((long long)nseq * hp.n, hp.cap))) nseq--;
-        k[2] = 0; k[3] = cT;
+        k[2] = 0; k[3] = cT * 64 + hp.emax;
     }
     return k;
 }
@@ -507,9 +516,9 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
         int capn[2] = {L.fr_cap, L.fc_cap};
         for (int d = 0; d < 2; d++) {
             const HostPlan& hp = *pl[d];
-            if (hp.n > MAX_FFT || hp.n > capn[d] || (int)hp.rad.size() > UNW_MAX_PASSES)
+            if (hp.n > MAX_GEN || hp.n > capn[d] || (int)hp.rad.size() > UNW_MAX_PASSES)
                 return set_err(UNW_E_UNSUPPORTED, "grid %d: transform length %d (from %d) exceeds %d", g, hp.n,
-                               hp.N, MAX_FFT);
+                               hp.N, MAX_GEN);
             DctPlanDev& D = *dp[d];
             D.N = hp.N;
             D.blue = hp.blue;
@@ -532,6 +541,8 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
         G.col_nseq = nseq;
         S.sh.row_T = std::max(S.sh.row_T, rT);
         S.sh.col_T = std::max(S.sh.col_T, cT);
+        S.sh.row_emax = std::max(S.sh.row_emax, prow[gi].emax);
+        S.sh.col_emax = std::max(S.sh.col_emax, pcol[gi].emax);
         S.sh.row_smem = std::max(S.sh.row_smem, (size_t)prow[gi].n * sizeof(float2));
         S.sh.col_smem = std::max(S.sh.col_smem, (size_t)nseq * pcol[gi].n * sizeof(float2));
         G.sten_tiles_x = (G.W + 127) / 128;
@@ -597,8 +608,8 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
         if (G.H == 0) continue;
         CK(unw_launch_tables(G.prow.fft, G.prow, const_cast<float*>(G.sW), G.W, s));
         CK(unw_launch_tables(G.pcol.fft, G.pcol, const_cast<float*>(G.sH), G.H, s));
-        if (G.prow.blue) CK(unw_launch_hspec(pick_threads(prow[g].n, prow[g].cap), EMAX, G.prow, s));
-        if (G.pcol.blue) CK(unw_launch_hspec(pick_threads(pcol[g].n, pcol[g].cap), EMAX, G.pcol, s));
+        if (G.prow.blue) CK(unw_launch_hspec(pick_threads(prow[g].n, prow[g].cap), prow[g].emax, G.prow, s));
+        if (G.pcol.blue) CK(unw_launch_hspec(pick_threads(pcol[g].n, pcol[g].cap), pcol[g].emax, G.pcol, s));
         CK(cudaMemsetAsync(G.hist, 0, sizeof(int) * HIST_CAP, s));
     }
 

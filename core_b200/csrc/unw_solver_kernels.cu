@@ -687,7 +687,7 @@ static cudaError_t launch_row_fwd_t(int T, int emax, dim3 grid, size_t smem, cud
         kfn<<<grid, TT, smem, s>>>(gd, st, n, it, cgk);                                     \
         return cudaGetLastError();                                                          \
     }
-    UNW_RF(128, 16) UNW_RF(256, 16) UNW_RF(512, 16) UNW_RF(1024, 16)
+    UNW_RF(128, 16) UNW_RF(256, 16) UNW_RF(512, 16) UNW_RF(1024, 16) UNW_RF(1024, 32)
 #undef UNW_RF
     return cudaErrorInvalidConfiguration;
 }
@@ -714,7 +714,7 @@ static cudaError_t launch_row_inv_t(int T, int emax, dim3 grid, size_t smem, cud
         kfn<<<grid, TT, smem, s>>>(gd, st, n);                                              \
         return cudaGetLastError();                                                          \
     }
-    UNW_RI(128, 16) UNW_RI(256, 16) UNW_RI(512, 16) UNW_RI(1024, 16)
+    UNW_RI(128, 16) UNW_RI(256, 16) UNW_RI(512, 16) UNW_RI(1024, 16) UNW_RI(1024, 32)
 #undef UNW_RI
     return cudaErrorInvalidConfiguration;
 }
@@ -741,7 +741,7 @@ static cudaError_t launch_col_t(int T, int emax, dim3 grid, size_t smem, cudaStr
         kfn<<<grid, TT, smem, s>>>(gd, st, n);                                              \
         return cudaGetLastError();                                                          \
     }
-    UNW_CL(128, 16) UNW_CL(256, 16) UNW_CL(512, 16) UNW_CL(1024, 16)
+    UNW_CL(128, 16) UNW_CL(256, 16) UNW_CL(512, 16) UNW_CL(1024, 16) UNW_CL(1024, 32)
 #undef UNW_CL
     return cudaErrorInvalidConfiguration;
 }
@@ -776,7 +776,7 @@ cudaError_t unw_launch_hspec(int T, int emax, const DctPlanDev& d, cudaStream_t 
         kfn<<<1, TT, smem, s>>>(d);                                                         \
         return cudaGetLastError();                                                          \
     }
-    UNW_HS(128, 16) UNW_HS(256, 16) UNW_HS(512, 16) UNW_HS(1024, 16)
+    UNW_HS(128, 16) UNW_HS(256, 16) UNW_HS(512, 16) UNW_HS(1024, 16) UNW_HS(1024, 32)
 #undef UNW_HS
     return cudaErrorInvalidConfiguration;
 }
