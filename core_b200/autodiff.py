@@ -12,7 +12,7 @@ from __future__ import annotations
 import ctypes as C
 
 from . import _lib
-from .unwrap2d import _torch, irls_unwrap_2d, make_params
+from .unwrap2d import _torch, irls_unwrap_2d, irls_unwrap_2d_batch, make_params
 
 
 def irls_adjoint(phase, weight, u, grad_u, *, cg_max_iter=1000, cg_tol=1e-6, epsilon=1e-2, need_weight=True):
@@ -51,7 +51,15 @@ def _make_function():
     class _Fn(torch.autograd.Function):
         @staticmethod
         def forward(ctx, phase, weight, kw, akw):
-            u, cc = irls_unwrap_2d(phase, weight, **kw)
+            if phase.ndim == 3:
+                # a batch of grids: one batched forward solve (each grid on its own tests)
+                ws = None if weight is None else list(weight)
+                res = irls_unwrap_2d_batch(list(phase), ws, **kw)
+                u = torch.stack([r[0] for r in res])
+                # labels stacked as int16, then reinterpreted
+                cc = torch.stack([r[1].view(torch.int16) for r in res]).view(res[0][1].dtype)
+            else:
+                u, cc = irls_unwrap_2d(phase, weight, **kw)
             ctx.save_for_backward(phase, weight if weight is not None else phase.new_empty(0), u)
             ctx.has_weight = weight is not None
             ctx.akw = akw
@@ -61,8 +69,17 @@ def _make_function():
         @staticmethod
         def backward(ctx, grad_u, grad_cc):
             phase, weight, u = ctx.saved_tensors
+            need_w = ctx.has_weight and ctx.needs_input_grad[1]
+            if phase.ndim == 3:
+                gphs, gws = [], []
+                for b in range(phase.shape[0]):
+                    w = weight[b] if ctx.has_weight else None
+                    gph, gw, _ = irls_adjoint(phase[b], w, u[b], grad_u[b], need_weight=need_w, **ctx.akw)
+                    gphs.append(gph)
+                    gws.append(gw)
+                return torch.stack(gphs), (torch.stack(gws) if need_w else None), None, None
             w = weight if ctx.has_weight else None
-            gph, gw, _ = irls_adjoint(phase, w, u, grad_u, need_weight=ctx.needs_input_grad[1], **ctx.akw)
+            gph, gw, _ = irls_adjoint(phase, w, u, grad_u, need_weight=need_w, **ctx.akw)
             return gph, gw, None, None
 
     return _Fn
@@ -75,6 +92,8 @@ def irls_unwrap_2d_diff(phase, weight=None, max_iter=50, tol=1e-3, cg_max_iter=2
                         conncomp_size=30, *, adjoint_cg_max_iter=1000, adjoint_cg_tol=1e-6):
     """`irls_unwrap_2d` on CUDA tensors with gradients for phase and weight.
 
+    phase (and weight): one (H, W) grid or a (B, H, W) batch (one batched forward
+    solve; one adjoint solve per grid in the backward pass).
     Returns (u, conncomp); u carries autograd history (conncomp does not).
     adjoint_cg_max_iter / adjoint_cg_tol control the backward pass's PCG solves
     (tolerance relative to each solve's initial residual).
@@ -83,6 +102,8 @@ def irls_unwrap_2d_diff(phase, weight=None, max_iter=50, tol=1e-3, cg_max_iter=2
     torch = _torch()
     if not (isinstance(phase, torch.Tensor) and phase.is_cuda):
         raise ValueError("irls_unwrap_2d_diff takes CUDA tensors")
+    if phase.ndim not in (2, 3):
+        raise ValueError(f"irls_unwrap_2d_diff expects (H, W) or (B, H, W), got {tuple(phase.shape)}")
     if _FN is None:
         _FN = _make_function()
     kw = dict(max_iter=max_iter, tol=tol, cg_max_iter=cg_max_iter, cg_tol=cg_tol, epsilon=epsilon,

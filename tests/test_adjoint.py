@@ -112,3 +112,27 @@ def test_autograd_function_backward():
     gph, gw, _ = core_b200.irls_adjoint(pt.detach(), ct.detach(), u.detach(), G)
     assert torch.allclose(pt.grad, gph, rtol=0, atol=1e-6 * float(gph.abs().max()))
     assert torch.allclose(ct.grad, gw, rtol=0, atol=1e-6 * float(gw.abs().max()) + 1e-30)
+
+
+@pytest.mark.gpu
+def test_autograd_batch_matches_single_grids():
+    torch = _gpu()
+    import core_b200
+    dev = torch.device("cuda", 0)
+    ps, cs, ts = zip(*[gen_g1(48, 56, seed=s, noise=1.0) for s in (21, 22, 23)])
+    pt = torch.from_numpy(np.stack(ps)).to(dev).requires_grad_(True)
+    ct = torch.from_numpy(np.stack(cs)).to(dev).requires_grad_(True)
+    tt = torch.from_numpy(np.stack(ts).astype(np.float32)).to(dev)
+    u, cc = core_b200.irls_unwrap_2d_diff(pt, ct)
+    assert u.shape == pt.shape and cc.shape == pt.shape
+    v = torch.isfinite(u)
+    (0.5 * (u[v] - tt[v]).pow(2).sum()).backward()
+    for b in range(3):
+        p1 = pt[b].detach().clone().requires_grad_(True)
+        c1 = ct[b].detach().clone().requires_grad_(True)
+        u1, _ = core_b200.irls_unwrap_2d_diff(p1, c1)
+        v1 = torch.isfinite(u1)
+        (0.5 * (u1[v1] - tt[b][v1]).pow(2).sum()).backward()
+        assert torch.allclose(u[b], u1, equal_nan=True)
+        assert torch.allclose(pt.grad[b], p1.grad, rtol=0, atol=1e-6 * float(p1.grad.abs().max()))
+        assert torch.allclose(ct.grad[b], c1.grad, rtol=0, atol=1e-6 * float(c1.grad.abs().max()) + 1e-30)
