@@ -283,8 +283,10 @@ def run_b200(args):
     # ---- end to end through the public API: pinned host input, numpy output
     pin_p = torch.from_numpy(p).pin_memory()
     pin_c = torch.from_numpy(c).pin_memory()
-    for _ in range(1):
-        core_b200.irls_unwrap_2d(pin_p, pin_c, device=dev, **FN)
+    # warm-up in the timed loop's own pattern: a caller that keeps the previous
+    # result while the next call runs holds two pinned output blocks
+    for _ in range(2):
+        u_np, cc_np = core_b200.irls_unwrap_2d(pin_p, pin_c, device=dev, **FN)
     torch.cuda.synchronize()
     barrier(world)
     e2e_steps = max(1, min(args.steps, 3))
