@@ -28,9 +28,9 @@ def load_golden(name):
 
 
 def small_golden_names():
-    """Unwrapper fixtures (L_* are the large ones, gs_* belong to the Goldstein filter)."""
+    """Unwrapper fixtures (L_* are the large ones; gs_* and lk_* belong to the filter and the linking)."""
     return sorted(f[:-4] for f in os.listdir(GOLDEN)
-                  if f.endswith(".npz") and not f.startswith("L_") and not f.startswith("gs_"))
+                  if f.endswith(".npz") and not f.startswith(("L_", "gs_", "lk_")))
 
 
 @pytest.fixture

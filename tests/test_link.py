@@ -1,0 +1,180 @@
+"""Component linking (insardev/insardev/utils_unwrap2d.py:195-444, :886-1040; Stack_unwrap2d.py:325-407).
+
+Golden fixtures: the reference's own linking functions run with stand-in
+geometry and CP-SAT modules (tests/golden/make_link_golden.py).  CPU tests pin
+the oracle to them and pin its primitives (border pixels against cv2 contours,
+hulls against qhull, the integer program against enumeration); GPU tests
+compare the CUDA path with the fixtures and the oracle.  The bar is exact:
+identical connection lists (indices, pixels, distances, window means) and
+bit-identical output rasters.
+"""
+import glob
+import itertools
+import os
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+from oracle import link_oracle as O
+
+GOLD = sorted(glob.glob(os.path.join(REPO, "tests", "golden", "lk_*.npz")))
+IDS = [os.path.basename(p)[:-4] for p in GOLD]
+
+
+def load(path):
+    d = np.load(path)
+    csize, gap, lsize, lcount = d["params"]
+    return dict(phase=d["phase"], conncomp=d["conncomp"] if bool(d["use_conncomp"]) else None,
+                conncomp_size=int(csize), conncomp_gap=None if gap < 0 else float(gap),
+                conncomp_linksize=int(lsize), conncomp_linkcount=int(lcount)), d
+
+
+def conn_array(conns):
+    return np.array([(c[0], c[1], c[2][0], c[2][1], c[3][0], c[3][1], c[4], c[5], float(c[6]), float(c[7]))
+                     for c in conns], np.float64).reshape(-1, 10)
+
+
+def same_raster(a, b):
+    na = np.isnan(a)
+    return np.array_equal(na, np.isnan(b)) and np.array_equal(a[~na], b[~na])
+
+
+def test_fixtures_present():
+    assert len(GOLD) >= 8
+
+
+@pytest.mark.parametrize("path", GOLD, ids=IDS)
+def test_oracle_matches_reference_fixture(path):
+    kw, d = load(path)
+    out, info = O.link(return_info=True, **kw)
+    np.testing.assert_array_equal(conn_array(info["connections"]), d["connections"])
+    assert same_raster(out, d["out"])
+
+
+def _random_labels(rng, H, W, p):
+    from scipy import ndimage
+    m = ndimage.binary_opening(rng.random((H, W)) < p) if rng.random() < 0.5 else rng.random((H, W)) < p
+    lab, n = ndimage.label(m, structure=O.STRUCT4)
+    return lab, n
+
+
+def test_border_pixels_equal_cv2_contours():
+    cv2 = pytest.importorskip("cv2")
+    from scipy import ndimage
+    rng = np.random.default_rng(0)
+    for _ in range(60):
+        H, W = rng.integers(5, 40, 2)
+        lab, n = _random_labels(rng, H, W, rng.uniform(0.4, 0.8))
+        for L in range(1, n + 1):
+            sl = ndimage.find_objects(lab)[L - 1]
+            cs, _ = cv2.findContours((lab[sl] == L).astype(np.uint8), cv2.RETR_TREE, cv2.CHAIN_APPROX_NONE)
+            pts = {(int(y) + sl[0].start, int(x) + sl[1].start) for c in cs for x, y in c.reshape(-1, 2)}
+            assert {tuple(p) for p in O.border_points(lab, L).tolist()} == pts
+
+
+def test_short_contours_are_straight_lines():
+    """The reference skips contours of < 3 points (utils_unwrap2d.py:240-241): one-row / one-column components."""
+    cv2 = pytest.importorskip("cv2")
+    from scipy import ndimage
+    rng = np.random.default_rng(1)
+    for _ in range(60):
+        H, W = rng.integers(5, 40, 2)
+        lab, n = _random_labels(rng, H, W, rng.uniform(0.3, 0.8))
+        for L in range(1, n + 1):
+            sl = ndimage.find_objects(lab)[L - 1]
+            cm = (lab[sl] == L).astype(np.uint8)
+            cs, _ = cv2.findContours(cm, cv2.RETR_TREE, cv2.CHAIN_APPROX_SIMPLE)
+            short = any(len(c) < 3 for c in cs)
+            assert short == (cm.shape[0] == 1 or cm.shape[1] == 1)
+
+
+def test_hull_matches_qhull():
+    from scipy.spatial import ConvexHull
+    rng = np.random.default_rng(2)
+    for _ in range(100):
+        pts = rng.integers(0, 50, (rng.integers(3, 60), 2))
+        if np.linalg.matrix_rank(pts - pts[0]) < 2:
+            continue
+        h = O.convex_hull(pts)
+        q = ConvexHull(pts[:, ::-1].astype(float))
+        assert set(h) == {tuple(int(v) for v in pts[k, ::-1]) for k in q.vertices}
+        n = len(h)
+        assert all(O._cross(h[k], h[(k + 1) % n], h[(k + 2) % n]) > 0 for k in range(n))
+
+
+def test_hull_distance_against_dense_sampling():
+    rng = np.random.default_rng(3)
+    for _ in range(40):
+        A = O.convex_hull(rng.integers(0, 30, (8, 2)))
+        B = O.convex_hull(rng.integers(0, 30, (8, 2)) + rng.integers(-20, 20, 2))
+        if len(A) < 3 or len(B) < 3:
+            continue
+        d = O.hull_distance(A, B)
+
+        def edge_pts(V):
+            t = np.linspace(0, 1, 200)[:, None]
+            return np.concatenate([np.array(V[k]) * (1 - t) + np.array(V[(k + 1) % len(V)]) * t
+                                   for k in range(len(V))])
+        ea, eb = edge_pts(A), edge_pts(B)
+        dd = np.sqrt(((ea[:, None] - eb[None]) ** 2).sum(-1)).min()
+        if d > 0:
+            assert abs(dd - d) <= 0.2
+        else:
+            # meeting: a vertex of one inside the other, or boundaries within sampling resolution
+            assert dd <= 0.2 or any(all(O._cross(B[k], B[(k + 1) % len(B)], p) >= 0 for k in range(len(B)))
+                                    for p in A) or any(all(O._cross(A[k], A[(k + 1) % len(A)], q) >= 0
+                                                           for k in range(len(A))) for q in B)
+
+
+def _enumerate(n, edges, sign, R=4):
+    best = None
+    s = 1 if sign == "reference" else -1
+    for ks in itertools.product(range(-R, R + 1), repeat=n - 1):
+        k = (0,) + ks
+        obj = sum(w * abs(s * (k[i] - k[j]) - off) for i, j, off, w in edges)
+        key = (obj, sum(abs(v) for v in k))
+        if best is None or key < best[0]:
+            best = (key, [k])
+        elif key == best[0]:
+            best[1].append(k)
+    return best
+
+
+@pytest.mark.parametrize("sign", ["reference", "aligned"])
+def test_offsets_program_matches_enumeration(sign):
+    rng = np.random.default_rng(4)
+    checked = 0
+    for _ in range(40):
+        n = int(rng.integers(2, 6))
+        m = int(rng.integers(1, 8))
+        edges = []
+        for _ in range(m):
+            i, j = sorted(rng.choice(n, 2, replace=False).tolist())
+            edges.append((i, j, int(rng.integers(-1, 2)), int(rng.integers(0, 3000))))
+        (obj, sec), sols = _enumerate(n, edges, sign)
+        k = O.solve_offsets(n, edges, sign)
+        s = 1 if sign == "reference" else -1
+        got = sum(w * abs(s * (k[i] - k[j]) - off) for i, j, off, w in edges)
+        assert got == obj and int(np.abs(k).sum()) == sec
+        if len(sols) == 1:
+            assert tuple(k.tolist()) == sols[0]
+            checked += 1
+    assert checked >= 20
+
+
+def test_aligned_sign_removes_offsets():
+    """With sign='aligned' three shifted blobs come back to one level; the reference sign does not."""
+    H, W = 40, 100
+    yy, xx = np.mgrid[:H, :W]
+    truth = (0.02 * xx).astype(np.float32)
+    ph = np.full((H, W), np.nan, np.float32)
+    for x0, m in ((5, 0), (38, 1), (71, -1)):
+        sl = (slice(10, 30), slice(x0, x0 + 24))
+        ph[sl] = truth[sl] + np.float32(2 * np.pi * m)
+    fixed = O.link(ph, conncomp_size=10, sign="aligned")
+    v = ~np.isnan(fixed)
+    # aligned to the first (largest) component: one constant 2-pi multiple everywhere
+    assert np.ptp(fixed[v] - truth[v]) < 1e-4
+    ref = O.link(ph, conncomp_size=10)
+    assert np.ptp(ref[v] - truth[v]) > 6.0
