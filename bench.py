@@ -145,10 +145,10 @@ def barrier(world):
 def make_input(seed=0, shape=None):
     """The 4096^2 G2 fault grid, or a G1 grid of the given (H, W) (seed + 1)."""
     if shape:
-        from oracle.generators import gen_g1
+        from core_b200.synthetic import gen_g1
         p, c, _ = gen_g1(int(shape[0]), int(shape[1]), seed=seed + 1)
         return p, c
-    from oracle.generators import gen_g2
+    from core_b200.synthetic import gen_g2
     p, c, _ = gen_g2(4096, seed=seed)
     return p, c
 
@@ -216,7 +216,7 @@ def run_b200(args):
 
     import core_b200
     from core_b200 import _lib
-    from core_b200.unwrap2d import make_params
+    from core_b200.irls import make_params
 
     rank, world, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
@@ -358,6 +358,11 @@ def run_b200(args):
                  "parallelism": f"grids sharded over {world} GPU(s)"}
         del sph, swt
 
+    # ---- component linking after the unwrap (Stack.unwrap2d's default path)
+    link = None
+    if not args.no_link_line:
+        link = link_measure(local, 3, 1)
+
     # ---- CPU baseline (rank 0, N=1 only): the oracle on a bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -380,7 +385,7 @@ def run_b200(args):
            "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(npx * 8),
                    "d2h_bytes_per_step": int(npx * 6)},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches // 1,
-           "stack": stack}
+           "stack": stack, "link": link}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
@@ -391,7 +396,7 @@ def run_b200(args):
 
 # --------------------------------------------------------------------------- stack workload
 def _gen_stack_entry(m):
-    from oracle.generators import gen_stack_grid
+    from core_b200.synthetic import gen_stack_grid
     p, c, _ = gen_stack_grid(m)
     return p, c
 
@@ -402,7 +407,7 @@ def stack_grids(n, rank, world):
     seeded metadata, so every rank computes the same shard without communicating."""
     import multiprocessing as mproc
     from core_b200.stack import shard_stack
-    from oracle.generators import gen_stack_meta
+    from core_b200.synthetic import gen_stack_meta
     meta = gen_stack_meta(n, seed=0)
     shapes = [(m[0], m[1]) for m in meta]
     mine = shard_stack(shapes, world)[rank]
@@ -411,13 +416,52 @@ def stack_grids(n, rank, world):
     return mine, [g[0] for g in grids], [g[1] for g in grids], sum(h * w for h, w in shapes)
 
 
+def link_measure(local, steps, warmup):
+    """Component linking on a 4096^2 scene of ~640 components >= 1000 px (the default conncomp_size of
+    Stack.unwrap2d): device-resident input, then numpy input and output (H2D + D2H inside)."""
+    import torch
+
+    import core_b200
+    from core_b200.synthetic import gen_link_scene
+    dev = torch.device("cuda", local)
+    ph, cc = gen_link_scene(4096, 4096, 2500, seed=110, holes=True, rmax=60)
+    tp = torch.from_numpy(ph).to(dev)
+    tc = torch.from_numpy(cc.view(np.int16)).to(dev)
+    kw = dict(conncomp_size=1000)
+    for _ in range(warmup):
+        core_b200.link_components(tp, tc, **kw)
+    torch.cuda.synchronize()
+    times, parts = [], []
+    for _ in range(steps):
+        t = time.perf_counter()
+        _, info = core_b200.link_components(tp, tc, return_info=True, **kw)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t)
+        parts.append(info["timing_ms"])
+    t_dev = float(np.median(times))
+    t = time.perf_counter()
+    for _ in range(steps):
+        core_b200.link_components(ph, cc, **kw)
+    t_e2e = (time.perf_counter() - t) / steps
+    npx = ph.size
+    return {"metric": "linked Mpx/s (4096^2, component linking)", "value": round(npx / 1e6 / t_dev, 2),
+            "unit": UNIT, "ms_per_step": round(t_dev * 1e3, 2), "steps": steps, "warmup": warmup,
+            "e2e": {"value": round(npx / 1e6 / t_e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(npx * 6),
+                    "d2h_bytes_per_step": int(npx * 4)},
+            "components": int(len(info["components"])), "connections": int(len(info["connections"])),
+            "ms_parts": {k: round(float(np.median([p[k] for p in parts])), 2) for k in parts[0]},
+            "timing": "host wall clock around each call (the call synchronises its stream)",
+            "workload": "gen_link_scene(4096, 4096, 2500 ellipses r<=60, holes, seed 110), conncomp_size 1000, "
+                        "linksize 5, linkcount 30, IRLS-style labels given"}
+
+
 def stack_measure(phases, weights, warmup, steps, world, local, npx_all):
     """Batched solves of this rank's grids, inputs resident in HBM: (Mpx/s over the whole
     stack, seconds per step (max over ranks), per-grid IRLS counts)."""
     import torch
 
     from core_b200 import _lib
-    from core_b200.unwrap2d import make_params
+    from core_b200.irls import make_params
 
     dev = torch.device("cuda", local)
     lib = _lib.load()
@@ -503,6 +547,8 @@ def main():
                     help="time a G1 grid of this shape instead of the 4096^2 fault grid")
     ap.add_argument("--no-stack-line", action="store_true",
                     help="leave the 64-grid stack sub-measurement out of the default line")
+    ap.add_argument("--no-link-line", action="store_true",
+                    help="leave the component-linking sub-measurement out of the default line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

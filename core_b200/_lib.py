@@ -57,6 +57,20 @@ class UnwStats(C.Structure):
                     prof_ms=list(self.prof_ms[:PROF_N]), prof_launches=list(self.prof_launches[:PROF_N]))
 
 
+UNW_LINK_C_LINE = 1
+
+
+class UnwLinkParams(C.Structure):
+    _fields_ = [("min_size", C.c_int32), ("max_neighbors", C.c_int32), ("window", C.c_int32), ("flags", C.c_int32)]
+
+
+class UnwLinkPair(C.Structure):
+    _fields_ = [("comp_i", C.c_int32), ("comp_j", C.c_int32), ("yi", C.c_int32), ("xi", C.c_int32),
+                ("yj", C.c_int32), ("xj", C.c_int32), ("d2", C.c_int64), ("blocked", C.c_int32),
+                ("n_i", C.c_int32), ("n_j", C.c_int32), ("nf_i", C.c_int32), ("nf_j", C.c_int32),
+                ("mean_i", C.c_float), ("mean_j", C.c_float), ("pad", C.c_int32)]
+
+
 class UnwGrid(C.Structure):
     _fields_ = [("phase", C.c_void_p), ("phase_pitch", C.c_int64), ("weight", C.c_void_p),
                 ("weight_pitch", C.c_int64), ("H", C.c_int64), ("W", C.c_int64),
@@ -87,6 +101,15 @@ SIGNATURES = {
     "unw_goldstein_c64": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
                                     C.c_int32, C.c_int32, C.c_float, C.c_void_p, C.c_int64, C.c_void_p,
                                     C.c_size_t, C.c_void_p]),
+    "unw_link_workspace_bytes": (C.c_size_t, [C.c_int64, C.c_int64, C.c_int32]),
+    "unw_link_pairs_f32": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
+                                     C.POINTER(UnwLinkParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                     C.POINTER(C.c_int32), C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
+                                     C.c_void_p, C.c_size_t, C.c_void_p]),
+    "unw_link_apply_f32": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_int32,
+                                     C.c_void_p, C.c_int64, C.c_void_p, C.c_size_t, C.c_int32, C.c_void_p]),
+    "unw_link_offsets": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_int32, C.c_void_p]),
     "unw_adjoint_f32": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
                                   C.POINTER(UnwParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
                                   C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_size_t,

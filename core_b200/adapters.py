@@ -12,7 +12,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .unwrap2d import irls_unwrap_2d, irls_unwrap_2d_batch
+from .irls import irls_unwrap_2d, irls_unwrap_2d_batch
 
 
 def _unpack(params_tuple):

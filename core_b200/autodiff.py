@@ -12,7 +12,7 @@ from __future__ import annotations
 import ctypes as C
 
 from . import _lib
-from .unwrap2d import _torch, irls_unwrap_2d, irls_unwrap_2d_batch, make_params
+from .irls import _torch, irls_unwrap_2d, irls_unwrap_2d_batch, make_params
 
 
 def irls_adjoint(phase, weight, u, grad_u, *, cg_max_iter=1000, cg_tol=1e-6, epsilon=1e-2, need_weight=True):

@@ -10,7 +10,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import _lib
-from .unwrap2d import _torch, resolve_device
+from .irls import _torch, resolve_device
 
 
 def goldstein(phase, corr, psize_y=32, psize_x=None, threshold=0.5, device='auto'):

@@ -48,7 +48,7 @@ def unwrap_stack(phases, weights=None, rank=0, world_size=1, device='auto', **kw
     Returns {grid index: (unwrapped, conncomp)} for the grids of this rank.
     Keyword arguments are those of `irls_unwrap_2d_batch`.
     """
-    from .unwrap2d import irls_unwrap_2d_batch
+    from .irls import irls_unwrap_2d_batch
     shapes = [tuple(p.shape) for p in phases]
     mine = shard_stack(shapes, world_size)[rank]
     if not mine:

@@ -1,6 +1,6 @@
-"""Seeded synthetic interferograms for parity tests and benchmarks.
+"""Seeded synthetic interferograms for parity tests, the benchmark and users.
 
-Test infrastructure only: nothing in the product package imports this module.
+Data only: the solver, linking and filter paths do not import this module.
 
 The reference ships no datasets for the unwrapper; its benchmark script builds
 synthetic wrapped phase with Gaussian/turbulent signals, decorrelation noise
@@ -20,6 +20,13 @@ G2  (`gen_g2`)   G1 plus a straight fault at a random angle through a point of t
 Stack (`gen_stack_meta`, `gen_stack_grid`)
                  64 G1 grids, rows U{1500..2600}, cols U{4000..7000},
                  noise sigma U[0.2, 0.8], grid i seeded with `seed * 1000 + i`.
+
+Link scene (`gen_link_scene`)
+                 n ellipses (centre U[0,H)xU[0,W), radii U[3, rmax]; with `holes`,
+                 30% lose their inner half-radius ellipse) as the valid mask; a
+                 smooth field plus N(0, noise^2), each 4-connected component shifted
+                 by 2*pi*U{-2..2}; labels numbered by size (1 = largest) as the
+                 unwrapper returns them.
 
 Draw order (G1): 8 x (amp, sigma, cy, cx); noise[H,W]; coherence[H,W];
 3 x (cy, cx, a0, b0, theta).  G2: 8 x (amp, sigma, cy, cx); fault (theta, py, px);
@@ -158,3 +165,30 @@ def gen_stack_meta(n=64, seed=0):
 def gen_stack_grid(meta_entry):
     rows, cols, sig, s = meta_entry
     return gen_g1(rows, cols, seed=s, noise=sig)
+
+
+def gen_link_scene(H, W, n_blobs, seed=0, holes=False, noise=0.15, rmax=None):
+    """Unwrapped phase with separately shifted components and their size-ordered uint16 labels."""
+    from scipy import ndimage
+    rng = np.random.default_rng(seed)
+    valid = np.zeros((H, W), bool)
+    for _ in range(n_blobs):
+        cy, cx = rng.uniform(0, H), rng.uniform(0, W)
+        ry, rx = rng.uniform(3, rmax or H / 8), rng.uniform(3, rmax or W / 8)
+        y0, y1 = max(0, int(cy - ry) - 1), min(H, int(cy + ry) + 2)
+        x0, x1 = max(0, int(cx - rx) - 1), min(W, int(cx + rx) + 2)
+        yy, xx = np.mgrid[y0:y1, x0:x1]
+        e = ((yy - cy) / ry) ** 2 + ((xx - cx) / rx) ** 2
+        valid[y0:y1, x0:x1] |= e <= 1.0
+        if holes and rng.random() < 0.3:
+            valid[y0:y1, x0:x1] &= ~(e <= 0.25)
+    lab, n = ndimage.label(valid, structure=[[0, 1, 0], [1, 1, 1], [0, 1, 0]])
+    yy, xx = np.mgrid[:H, :W]
+    truth = 0.03 * yy - 0.02 * xx + 2.0 * np.sin(xx / 37.0) * np.cos(yy / 53.0)
+    shift = 2 * np.pi * rng.integers(-2, 3, n + 1)
+    ph = np.where(valid, truth + shift[lab] + rng.normal(0, noise, (H, W)), np.nan).astype(np.float32)
+    sizes = np.bincount(lab.ravel(), minlength=n + 1)
+    order = sorted(range(1, n + 1), key=lambda L: (-sizes[L], -L))
+    lut = np.zeros(n + 1, np.uint16)
+    lut[order] = np.arange(1, n + 1)
+    return ph, lut[lab]

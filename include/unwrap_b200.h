@@ -212,6 +212,74 @@ UNW_API int unw_goldstein_c64(const float* phase, int64_t phase_pitch, const flo
                               void* cuda_stream);
 
 /*
+ * Component linking: integer 2-pi offsets between separately unwrapped
+ * components.  Replaces the geometry of find_component_connections_fast
+ * (insardev/insardev/utils_unwrap2d.py:195-444) and the raster updates of
+ * connect_components_ilp_fast (:886-1040), as driven by _link_2d
+ * (Stack_unwrap2d.py:325-407); the reference's cv2 contours and shapely
+ * measures become pixel-lattice geometry (boundary = border pixels, polygon =
+ * their convex hull, distances between pixel centres).  The greedy choice of
+ * connections and the integer program run on the host between the two calls.
+ *
+ * unw_link_pairs_f32: components from labels (uint16 IRLS labels, label
+ * order; NULL = 4-connected components of the non-NaN pixels, size order),
+ * kept when they have >= min_size pixels; then every candidate pair (each
+ * component with its max_neighbors nearest by hull distance) with its closest
+ * border pixels, whether the segment between them meets a third component's
+ * hull, and np.nanmean of each side's values in a (2*(window/2)+1)^2 window.
+ * Outputs go to host arrays; when comp_cap or pair_cap is too small the call
+ * returns UNW_E_WORKSPACE with the needed counts in *n_comp / *n_pairs.
+ * For the mask path comp_label holds the raster index of the component's
+ * first pixel.  The workspace keeps the component raster for
+ * unw_link_apply_f32, which writes phase + 2*pi*k[c] on component c, NaN on
+ * labelled pixels of components below min_size, and phase elsewhere; call it
+ * with the same workspace, shape and min_size.
+ */
+typedef struct unw_link_params {
+    int32_t min_size;       /* the reference uses max(conncomp_size, 4)             */
+    int32_t max_neighbors;  /* conncomp_linkcount (<= 256 unless >= components - 1) */
+    int32_t window;         /* conncomp_linksize, 0..31                             */
+    int32_t flags;          /* reserved, 0                                          */
+} unw_link_params;
+
+#define UNW_LINK_C_LINE 1   /* component in one row or column: no contour polygon */
+
+typedef struct unw_link_pair {
+    int32_t comp_i, comp_j;       /* component indices, comp_i < comp_j             */
+    int32_t yi, xi, yj, xj;       /* closest border pixels (ties: smallest yi,xi,yj,xj) */
+    int64_t d2;                   /* their squared distance                          */
+    int32_t blocked;              /* the segment meets a third component's hull      */
+    int32_t n_i, n_j;             /* window pixels of each component                 */
+    int32_t nf_i, nf_j;           /* ... of which finite                             */
+    float mean_i, mean_j;         /* np.nanmean of the window values (NaN if none)   */
+    int32_t pad;
+} unw_link_pair;
+
+UNW_API size_t unw_link_workspace_bytes(int64_t H, int64_t W, int32_t min_size);
+UNW_API int unw_link_pairs_f32(const float* phase, int64_t phase_pitch,
+                               const uint16_t* labels, int64_t label_pitch,
+                               int64_t H, int64_t W, const unw_link_params* params,
+                               int64_t* comp_label, int64_t* comp_size, int32_t* comp_flags,
+                               int32_t comp_cap, int32_t* n_comp,
+                               unw_link_pair* pairs, int32_t pair_cap, int32_t* n_pairs,
+                               void* workspace, size_t workspace_bytes, void* cuda_stream);
+UNW_API int unw_link_apply_f32(const float* phase, int64_t phase_pitch, int64_t H, int64_t W,
+                               const int32_t* k, int32_t n_comp, float* out, int64_t out_pitch,
+                               void* workspace, size_t workspace_bytes, int32_t min_size,
+                               void* cuda_stream);
+
+/*
+ * Integer offsets for the linking connections (host code, no GPU): the program
+ * connect_components_ilp_fast gives to CP-SAT (utils_unwrap2d.py:933-970),
+ * minimise sum_e w[e] |s (k[ei[e]] - k[ej[e]]) - off[e]| with k[0] = 0,
+ * k in [-100, 100], |s (k_i - k_j) - off| <= 200, s = +1 (sign >= 0, the
+ * reference) or -1; among optimal assignments the least sum |k| (exact).
+ * w[e] in [0, 2^31], off[e] in [-200, 200].  Writes k_out[0..n).
+ */
+UNW_API int unw_link_offsets(int32_t n, int32_t m, const int32_t* ei, const int32_t* ej, const int32_t* off,
+                             const int64_t* w, int32_t sign, int32_t* k_out);
+
+/*
  * Allocation-free variant of unw_apply_preconditioner.  It has no counterpart
  * in the reference.  It is for callers that cannot allocate device memory
  * where they need the operator (inside another framework's graph capture or

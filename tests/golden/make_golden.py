@@ -40,7 +40,7 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 sys.path.insert(0, HERE)
 
-from oracle.generators import gen_g1, gen_g2  # noqa: E402
+from core_b200.synthetic import gen_g1, gen_g2  # noqa: E402
 
 FN_DEFAULTS = dict(max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2, conncomp_size=30)
 API_DEFAULTS = dict(max_iter=50, tol=1e-2, cg_max_iter=10, cg_tol=1e-3, epsilon=1e-2, conncomp_size=30)

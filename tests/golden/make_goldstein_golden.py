@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 
-from oracle.generators import gen_g1  # noqa: E402
+from core_b200.synthetic import gen_g1  # noqa: E402
 
 
 def load_reference(ref_root):

@@ -119,7 +119,7 @@ def _gpu():
 def test_tiled_unwrap_equals_per_tile_solves():
     _gpu()
     import core_b200
-    from oracle.generators import gen_g1
+    from core_b200.synthetic import gen_g1
     p, c, _ = gen_g1(300, 260, seed=31)
     w = np.stack([c, c])
     ps = np.stack([p, gen_g1(300, 260, seed=32)[0]])
@@ -140,7 +140,7 @@ def test_tiled_unwrap_equals_per_tile_solves():
 def test_tiled_unwrap_matches_oracle_per_tile():
     _gpu()
     import core_b200
-    from oracle.generators import gen_g1
+    from core_b200.synthetic import gen_g1
     from oracle.irls_oracle import cycle_map, irls_unwrap_2d as oracle_unwrap
     p, c, _ = gen_g1(200, 180, seed=33)
     out = core_b200.unwrap2d_chunk(p, c, chunks=(100, 90), overlap=12)
@@ -162,7 +162,7 @@ def test_tiled_unwrap_matches_oracle_per_tile():
 def test_overlap_kernel_matches_single_solves():
     _gpu()
     import core_b200
-    from oracle.generators import gen_g1, gen_g2
+    from core_b200.synthetic import gen_g1, gen_g2
     blk = np.stack([gen_g1(96, 112, seed=41)[0], np.full((96, 112), np.nan), gen_g2(96, 112, seed=42)[0]])
     out = adapters._irls_overlap_kernel(blk, PARAMS)
     assert np.isnan(out[1]).all()

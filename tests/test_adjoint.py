@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from oracle.adjoint_oracle import Frozen
-from oracle.generators import gen_g1
+from core_b200.synthetic import gen_g1
 from oracle.irls_oracle import irls_unwrap_2d as oracle_unwrap
 
 

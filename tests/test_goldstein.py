@@ -83,7 +83,7 @@ def test_cuda_matches_reference_fixture(path):
 def test_cuda_matches_oracle_larger_and_tensor_io():
     torch = _gpu()
     import core_b200
-    from oracle.generators import gen_g1
+    from core_b200.synthetic import gen_g1
     p, c, _ = gen_g1(300, 257, seed=9, noise=0.7)
     z = np.exp(1j * p.astype(np.float64)).astype(np.complex64)
     z[np.isnan(p)] = np.nan

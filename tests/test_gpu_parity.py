@@ -19,7 +19,7 @@ import pytest
 import scipy.fft as sfft
 
 from conftest import load_golden, small_golden_names
-from oracle.generators import gen_g1, gen_g2
+from core_b200.synthetic import gen_g1, gen_g2
 from oracle.irls_oracle import cycle_map, irls_unwrap_2d as oracle_unwrap
 
 torch = pytest.importorskip("torch")
@@ -323,7 +323,7 @@ def test_repeat_calls_on_reused_workspace_are_identical():
     # the second call reuses the first call's workspace (stale contents must not matter)
     p, c, _ = gen_g1(1024, seed=0)
     u1, c1 = core_b200.irls_unwrap_2d(p, c)
-    ws = core_b200.unwrap2d._ws().buf
+    ws = core_b200.irls._ws().buf
     for b in ws.values():
         b.fill_(0xA5)                       # poison the cached workspace
     u2, c2 = core_b200.irls_unwrap_2d(p, c)
@@ -332,7 +332,7 @@ def test_repeat_calls_on_reused_workspace_are_identical():
 
 
 def _solve_flags(p, c, flags, **kw):
-    from core_b200.unwrap2d import make_params
+    from core_b200.irls import make_params
     lib = _lib.load()
     H, W = p.shape
     ph = torch.from_numpy(np.ascontiguousarray(p, np.float32)).to(DEV)

@@ -153,14 +153,29 @@ def test_offsets_program_matches_enumeration(sign):
             i, j = sorted(rng.choice(n, 2, replace=False).tolist())
             edges.append((i, j, int(rng.integers(-1, 2)), int(rng.integers(0, 3000))))
         (obj, sec), sols = _enumerate(n, edges, sign)
-        k = O.solve_offsets(n, edges, sign)
+        from core_b200.link import solve_offsets as native
         s = 1 if sign == "reference" else -1
-        got = sum(w * abs(s * (k[i] - k[j]) - off) for i, j, off, w in edges)
-        assert got == obj and int(np.abs(k).sum()) == sec
-        if len(sols) == 1:
-            assert tuple(k.tolist()) == sols[0]
-            checked += 1
+        for k in (O.solve_offsets(n, edges, sign), native(n, edges, sign)):
+            got = sum(w * abs(s * (k[i] - k[j]) - off) for i, j, off, w in edges)
+            assert got == obj and int(np.abs(k).sum()) == sec
+            if len(sols) == 1:
+                assert tuple(k.tolist()) == sols[0]
+        checked += len(sols) == 1
     assert checked >= 20
+
+
+def test_native_offsets_match_milp_on_large_programs():
+    """The library's exact solver (unw_link_offsets, no GPU) against the oracle's HiGHS MILP."""
+    from core_b200.link import solve_offsets as native
+    rng = np.random.default_rng(5)
+    for n, m in ((40, 150), (200, 900)):
+        edges = []
+        while len(edges) < m:
+            i, j = (int(v) for v in rng.integers(0, n, 2))
+            if i != j:
+                edges.append((min(i, j), max(i, j), int(rng.integers(-3, 4)), int(rng.integers(0, 2_000_000))))
+        for sign in ("reference", "aligned"):
+            np.testing.assert_array_equal(native(n, edges, sign), O.solve_offsets(n, edges, sign))
 
 
 def test_aligned_sign_removes_offsets():
@@ -178,3 +193,129 @@ def test_aligned_sign_removes_offsets():
     assert np.ptp(fixed[v] - truth[v]) < 1e-4
     ref = O.link(ph, conncomp_size=10)
     assert np.ptp(ref[v] - truth[v]) > 6.0
+
+
+# ------------------------------------------------------------------ GPU
+def _gpu():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _scene(seed, H, W, n_blobs, holes=False, noise=0.15, rmax=None):
+    from core_b200.synthetic import gen_link_scene
+    return gen_link_scene(H, W, n_blobs, seed=seed, holes=holes, noise=noise, rmax=rmax)
+
+
+def _check_cuda_vs(kw, ref_conns, ref_out):
+    import core_b200
+    out, info = core_b200.link_components(return_info=True, **kw)
+    assert out.dtype == np.float32 and out.shape == kw["phase"].shape
+    np.testing.assert_array_equal(conn_array(info["connections"]), ref_conns)
+    assert same_raster(out, ref_out)
+    return info
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", GOLD, ids=IDS)
+def test_cuda_matches_reference_fixture(path):
+    _gpu()
+    kw, d = load(path)
+    _check_cuda_vs(kw, d["connections"], d["out"])
+
+
+CASES = [
+    # seed, H, W, blobs, holes, use labels, conncomp_size, gap, linksize, linkcount
+    (101, 160, 200, 14, False, True, 30, None, 5, 30),
+    (102, 160, 200, 14, True, False, 30, None, 5, 30),
+    (103, 200, 180, 24, True, True, 20, None, 5, 2),
+    (104, 220, 260, 30, False, False, 40, 15.0, 7, 3),
+    (105, 128, 333, 18, True, True, 10, 25.0, 3, 1),
+    (106, 300, 301, 40, True, True, 60, None, 9, 4),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", CASES, ids=[str(c[0]) for c in CASES])
+def test_cuda_matches_oracle(case):
+    _gpu()
+    seed, H, W, nb, holes, use_cc, csize, gap, lsize, lcount = case
+    ph, cc = _scene(seed, H, W, nb, holes)
+    kw = dict(phase=ph, conncomp=cc if use_cc else None, conncomp_size=csize, conncomp_gap=gap,
+              conncomp_linksize=lsize, conncomp_linkcount=lcount)
+    ref, rinfo = O.link(return_info=True, **kw)
+    info = _check_cuda_vs(kw, conn_array(rinfo["connections"]), ref)
+    assert len(info["components"]) == len(rinfo["components"])
+    if not use_cc:
+        assert list(info["sizes"]) == [int((np.asarray(O.components_from_mask(~np.isnan(ph), max(csize, 4))[0])
+                                             == L).sum()) for L in rinfo["components"]]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sign", ["reference", "aligned"])
+def test_cuda_sign_and_tensor_io(sign):
+    torch = _gpu()
+    import core_b200
+    ph, cc = _scene(107, 150, 170, 12, False)
+    ref = O.link(ph, cc, conncomp_size=30, sign=sign)
+    dev = torch.device("cuda", 0)
+    t = core_b200.link_components(torch.from_numpy(ph).to(dev), torch.from_numpy(cc.astype(np.int32)).to(dev),
+                                  conncomp_size=30, sign=sign)
+    assert t.is_cuda and t.dtype == torch.float32
+    assert same_raster(t.cpu().numpy(), ref)
+    out3 = core_b200.link_components(ph[None], cc[None], conncomp_size=30, sign=sign)
+    assert out3.shape == (1,) + ph.shape and same_raster(out3[0], ref)
+
+
+@pytest.mark.gpu
+def test_cuda_edge_cases():
+    _gpu()
+    import core_b200
+    allnan = np.full((20, 30), np.nan, np.float32)
+    assert np.isnan(core_b200.link_components(allnan)).all()
+    one = np.zeros((20, 30), np.float32)
+    assert same_raster(core_b200.link_components(one), one)
+    # a small labelled component is removed, label 0 pixels are kept
+    ph, cc = _scene(108, 80, 90, 6, False)
+    cc2 = cc.copy()
+    cc2[cc == cc.max()] = 0
+    for kw in (dict(conncomp=cc2, conncomp_size=10 ** 6), dict(conncomp=cc, conncomp_size=50)):
+        out = core_b200.link_components(ph, **kw)
+        assert same_raster(out, O.link(ph, **kw))
+
+
+@pytest.mark.gpu
+def test_unwrap2d_links_irls_components():
+    _gpu()
+    import core_b200
+    ph, _ = _scene(109, 180, 240, 12, False, noise=0.3)
+    wrapped = np.angle(np.exp(1j * ph.astype(np.float64))).astype(np.float32)
+    wrapped[np.isnan(ph)] = np.nan
+    u, cc = core_b200.unwrap2d(wrapped, conncomp=True, conncomp_size=50)
+    out = core_b200.unwrap2d(wrapped, conncomp_size=50)
+    assert same_raster(out, O.link(u, cc, conncomp_size=50))
+    stack = core_b200.unwrap2d(np.stack([wrapped, wrapped]), conncomp_size=50)
+    assert stack.shape == (2,) + wrapped.shape and same_raster(stack[1], out)
+    with pytest.raises(ValueError):
+        core_b200.unwrap2d(wrapped, conncomp_size=4, conncomp_linksize=5)
+
+
+@pytest.mark.gpu
+def test_cuda_large_grid_properties():
+    """2048^2 with a few hundred components: each component moves by one 2-pi multiple, the first stays."""
+    _gpu()
+    import core_b200
+    ph, cc = _scene(110, 2048, 2048, 600, True, rmax=45)
+    out, info = core_b200.link_components(ph, cc, conncomp_size=200, return_info=True)
+    comps = info["components"]
+    assert len(comps) > 50 and len(info["connections"]) > len(comps) // 2
+    d = (out.astype(np.float64) - ph) / (2 * np.pi)
+    for c, L in enumerate(comps[:60]):
+        m = cc == L
+        kd = np.unique(np.round(d[m]))
+        assert len(kd) == 1 and kd[0] == info["k"][c]
+        assert np.abs(d[m] - kd[0]).max() < 1e-5
+    assert info["k"][0] == 0
+    small = (cc > 0) & ~np.isin(cc, comps)
+    assert np.isnan(out[small]).all()

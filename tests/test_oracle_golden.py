@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from conftest import load_golden, small_golden_names
-from oracle.generators import gen_g1, gen_g2
+from core_b200.synthetic import gen_g1, gen_g2
 from oracle.irls_oracle import OracleStats, cycle_map, irls_unwrap_2d
 
 

@@ -14,7 +14,7 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 from core_b200.stack import shard_stack
-from oracle.generators import gen_stack_meta
+from core_b200.synthetic import gen_stack_meta
 
 
 def test_shard_single_rank_takes_everything():
