@@ -156,6 +156,51 @@ struct Program {
     }
 };
 
+// Starting point: every edge of a maximum-weight spanning forest satisfied
+// exactly (k_0 = 0, the first node of every other tree at 0).  Only shortens the
+// descent; the descent then reaches the minimum from here.  Falls back to zero
+// when the start leaves the bounds.
+std::vector<int> spanning_start(const Program& P) {
+    const int n = P.n, m = P.m;
+    std::vector<int> order(m);
+    for (int e = 0; e < m; e++) order[e] = e;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return P.w[a] > P.w[b]; });
+    std::vector<int> root(n);
+    for (int v = 0; v < n; v++) root[v] = v;
+    auto find = [&](int v) { while (root[v] != v) v = root[v] = root[root[v]]; return v; };
+    std::vector<std::vector<std::pair<int, int>>> adj(n);   // (neighbour, edge)
+    for (int e : order) {
+        const int a = find(P.ei[e]), b = find(P.ej[e]);
+        if (a == b) continue;
+        root[std::max(a, b)] = std::min(a, b);
+        adj[P.ei[e]].push_back({P.ej[e], e});
+        adj[P.ej[e]].push_back({P.ei[e], e});
+    }
+    std::vector<int> k(n, 0);
+    std::vector<char> seen(n, 0);
+    for (int r = 0; r < n; r++) {
+        if (seen[r]) continue;
+        seen[r] = 1;
+        std::vector<int> st{r};
+        while (!st.empty()) {
+            const int u = st.back(); st.pop_back();
+            for (auto [v, e] : adj[u]) {
+                if (seen[v]) continue;
+                seen[v] = 1;
+                // s (k_i - k_j) = off[e]
+                if (P.ei[e] == u) k[v] = k[u] - P.s * P.off[e];
+                else k[v] = k[u] + P.s * P.off[e];
+                st.push_back(v);
+            }
+        }
+    }
+    for (int v = 0; v < n; v++)
+        if (k[v] < -100 || k[v] > 100) return std::vector<int>(n, 0);
+    for (int e = 0; e < m; e++)
+        if (std::llabs((int64_t)P.s * (k[P.ei[e]] - k[P.ej[e]]) - P.off[e]) > 200) return std::vector<int>(n, 0);
+    return k;
+}
+
 }  // namespace
 
 extern "C" int unw_link_offsets(int32_t n, int32_t m, const int32_t* ei, const int32_t* ej, const int32_t* off,
@@ -171,6 +216,7 @@ extern "C" int unw_link_offsets(int32_t n, int32_t m, const int32_t* ei, const i
     std::vector<int> k(n, 0);
     if (n >= 2 && m > 0) {
         Program P{n, m, ei, ej, off, w, sign >= 0 ? 1 : -1, (Cap)100 * n + 1};
+        k = spanning_start(P);
         Cap f = P.objective(k);
         for (int iter = 0; iter < 1000; iter++) {
             Cap best = f;

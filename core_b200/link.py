@@ -121,6 +121,41 @@ def _device_labels(conncomp, dev, H, W):
     return t
 
 
+def _device_pairs(ph, lab, min_size, K, window, dev, stream):
+    """unw_link_pairs_f32 on device tensors: (labels, sizes, pair array, pair count, workspace)."""
+    lib = _lib.load()
+    H, W = int(ph.shape[0]), int(ph.shape[1])
+    prm = _lib.UnwLinkParams(min_size, K, window, 0)
+    ws = _ws().get(dev, lib.unw_link_workspace_bytes(H, W, min_size))
+    ncomp, npair = C.c_int32(0), C.c_int32(0)
+    ccap, pcap = 1024, 1024 * max(K, 1)
+    for _ in range(2):
+        clab = np.zeros(ccap, np.int64)
+        csz = np.zeros(ccap, np.int64)
+        cfl = np.zeros(ccap, np.int32)
+        pairs = (_lib.UnwLinkPair * max(pcap, 1))()
+        rc = lib.unw_link_pairs_f32(ph.data_ptr(), W, lab.data_ptr() if lab is not None else None, W, H, W,
+                                    C.byref(prm), clab.ctypes.data, csz.ctypes.data, cfl.ctypes.data, ccap,
+                                    C.byref(ncomp), pairs, pcap, C.byref(npair), ws.data_ptr(), ws.numel(), stream)
+        if rc == _lib.UNW_E_WORKSPACE and (ncomp.value > ccap or npair.value > pcap):
+            ccap, pcap = max(ccap, ncomp.value), max(pcap, npair.value)
+            continue
+        _lib.check(rc, "unw_link_pairs_f32")
+        break
+    n = ncomp.value
+    return clab[:n].copy(), csz[:n].copy(), pairs, npair.value, ws
+
+
+def _edge_weights(conns, sizes):
+    """(i, j, k_offset, int(1000 * weight)) per connection (utils_unwrap2d.py:917-931, :956-962)."""
+    edges = []
+    for ci, cj, _, _, dist, k_off, conf, _ in conns:
+        size_weight = np.sqrt(min(sizes[ci], sizes[cj]))
+        weight = conf * size_weight / (np.sqrt(dist) + 1.0)
+        edges.append((ci, cj, int(k_off), int(weight * 1000)))
+    return edges
+
+
 def link_components(phase, conncomp=None, conncomp_size=100, conncomp_gap=None, conncomp_linksize=5,
                     conncomp_linkcount=30, debug=False, *, device='auto', sign='reference', return_info=False):
     """Link separately unwrapped components by integer 2-pi offsets (`_link_2d`, Stack_unwrap2d.py:325-407).
@@ -143,7 +178,6 @@ def link_components(phase, conncomp=None, conncomp_size=100, conncomp_gap=None, 
         raise ValueError(f"link_components expects a 2D phase array, got shape {tuple(phase.shape)}")
     H, W = int(ph2.shape[0]), int(ph2.shape[1])
     dev = resolve_device(device, ph2)
-    lib = _lib.load()
     info = {"components": np.zeros(0, np.int64), "sizes": np.zeros(0, np.int64), "connections": [],
             "k": np.zeros(0, np.int64)}
 
@@ -166,41 +200,20 @@ def link_components(phase, conncomp=None, conncomp_size=100, conncomp_gap=None, 
         lab = _device_labels(cc2, dev, H, W) if cc2 is not None else None
         min_size = max(int(conncomp_size), 4)
         K = int(conncomp_linkcount)
-        prm = _lib.UnwLinkParams(min_size, K, int(conncomp_linksize), 0)
-        ws = _ws().get(dev, lib.unw_link_workspace_bytes(H, W, min_size))
         stream = torch.cuda.current_stream(dev).cuda_stream
-        ncomp, npair = C.c_int32(0), C.c_int32(0)
-        ccap, pcap = 1024, 1024 * max(K, 1)
         t0 = time.perf_counter()
-        for _ in range(2):
-            clab = np.zeros(ccap, np.int64)
-            csz = np.zeros(ccap, np.int64)
-            cfl = np.zeros(ccap, np.int32)
-            pairs = (_lib.UnwLinkPair * max(pcap, 1))()
-            rc = lib.unw_link_pairs_f32(ph.data_ptr(), W, lab.data_ptr() if lab is not None else None, W, H, W,
-                                        C.byref(prm), clab.ctypes.data, csz.ctypes.data, cfl.ctypes.data, ccap,
-                                        C.byref(ncomp), pairs, pcap, C.byref(npair), ws.data_ptr(), ws.numel(),
-                                        stream)
-            if rc == _lib.UNW_E_WORKSPACE and (ncomp.value > ccap or npair.value > pcap):
-                ccap, pcap = max(ccap, ncomp.value), max(pcap, npair.value)
-                continue
-            _lib.check(rc, "unw_link_pairs_f32")
-            break
-        n = ncomp.value
+        clab, csz, pairs, npair, ws = _device_pairs(ph, lab, min_size, K, int(conncomp_linksize), dev, stream)
+        n = len(clab)
         t1 = time.perf_counter()
-        info["components"], info["sizes"] = clab[:n].copy(), csz[:n].copy()
+        info["components"], info["sizes"] = clab, csz
         k = np.zeros(n, np.int32)
         t2 = t1
         if n >= 2:
-            conns = _greedy_connections(pairs, npair.value, K, conncomp_gap)
+            conns = _greedy_connections(pairs, npair, K, conncomp_gap)
             info["connections"] = conns
             t2 = time.perf_counter()
             if conns:
-                edges = []
-                for ci, cj, _, _, dist, k_off, conf, _ in conns:
-                    size_weight = np.sqrt(min(csz[ci], csz[cj]))
-                    weight = conf * size_weight / (np.sqrt(dist) + 1.0)
-                    edges.append((ci, cj, int(k_off), int(weight * 1000)))
+                edges = _edge_weights(conns, csz)
                 kk = solve_offsets(n, edges, sign)
                 kk[~_reachable_from_first(n, edges)] = 0
                 k = kk.astype(np.int32)
@@ -210,8 +223,8 @@ def link_components(phase, conncomp=None, conncomp_size=100, conncomp_gap=None, 
                   f"{int(np.count_nonzero(k))} offsets applied")
         t3 = time.perf_counter()
         out = torch.empty((H, W), dtype=torch.float32, device=dev)
-        rc = lib.unw_link_apply_f32(ph.data_ptr(), W, H, W, k.ctypes.data, n, out.data_ptr(), W, ws.data_ptr(),
-                                    ws.numel(), min_size, stream)
+        rc = _lib.load().unw_link_apply_f32(ph.data_ptr(), W, H, W, k.ctypes.data, n, out.data_ptr(), W,
+                                            ws.data_ptr(), ws.numel(), min_size, stream)
         _lib.check(rc, "unw_link_apply_f32")
         info["timing_ms"] = {"geometry": 1e3 * (t1 - t0), "greedy": 1e3 * (t2 - t1), "offsets": 1e3 * (t3 - t2),
                              "apply": 1e3 * (time.perf_counter() - t3)}
@@ -219,36 +232,101 @@ def link_components(phase, conncomp=None, conncomp_size=100, conncomp_gap=None, 
 
 
 def _greedy_connections(pairs, npair, max_neighbors, gap):
-    """Connections in order of distance under the per-component cap (utils_unwrap2d.py:335-444)."""
-    P = np.ctypeslib.as_array(pairs, shape=(max(npair, 1),))[:npair] if npair else []
-    cand = []
-    for p in P:
-        if p["blocked"]:
-            continue
-        dist = math.sqrt(float(p["d2"]))
-        if gap is not None and dist > gap:
-            continue
-        cand.append((dist, int(p["comp_i"]), int(p["comp_j"]), p))
-    cand.sort(key=lambda v: (v[0], v[1], v[2]))
-    count = {}
+    """Connections in order of distance under the per-component cap (utils_unwrap2d.py:335-444).
+
+    Filter, sort and the float32 offset arithmetic run on whole columns (numpy float32 arrays round
+    each operation as the reference's numpy float32 scalars do); only the cap walk is a loop.
+    """
+    if npair == 0:
+        return []
+    P = np.ctypeslib.as_array(pairs, shape=(len(pairs),))[:npair]
+    dist = np.sqrt(P["d2"].astype(np.float64))
+    keep = P["blocked"] == 0
+    if gap is not None:
+        keep &= ~(dist > gap)
+    idx = np.nonzero(keep)[0]
+    ci, cj = P["comp_i"][idx].astype(np.int64), P["comp_j"][idx].astype(np.int64)
+    order = np.lexsort((cj, ci, dist[idx]))
+    idx, ci, cj = idx[order], ci[order], cj[order]
+    mi, mj = P["mean_i"][idx], P["mean_j"][idx]
+    usable = (P["n_i"][idx] > 0) & (P["n_j"][idx] > 0) & ~np.isnan(mi) & ~np.isnan(mj)
+    delta = mi - mj                                            # float32
+    q = delta / (2 * np.pi)                                    # float32 / Python float -> float32
+    k_off = np.round(q)                                        # half to even, float32
+    fractional = q - k_off                                     # float32 - float32
+    confidence = np.maximum(np.float32(0), np.float32(1.0) - np.float32(2) * np.abs(fractional))
     conns = []
-    for dist, i, j, p in cand:
-        if count.get(i, 0) >= max_neighbors or count.get(j, 0) >= max_neighbors:
+    count = {}
+    ci_l, cj_l, idx_l, use_l = ci.tolist(), cj.tolist(), idx.tolist(), usable.tolist()
+    for t in range(len(idx_l)):
+        i, j = ci_l[t], cj_l[t]
+        if count.get(i, 0) >= max_neighbors or count.get(j, 0) >= max_neighbors or not use_l[t]:
             continue
-        if p["n_i"] == 0 or p["n_j"] == 0:
-            continue
-        mean_i, mean_j = np.float32(p["mean_i"]), np.float32(p["mean_j"])
-        if np.isnan(mean_i) or np.isnan(mean_j):
-            continue
-        delta = mean_i - mean_j
-        k_offset = int(np.round(delta / (2 * np.pi)))
-        fractional = (delta / (2 * np.pi)) - k_offset
-        confidence = max(0, 1.0 - 2 * abs(fractional))
-        conns.append((i, j, (int(p["yi"]), int(p["xi"])), (int(p["yj"]), int(p["xj"])), dist, k_offset,
-                      confidence, delta))
+        p = P[idx_l[t]]
+        conf = confidence[t] if confidence[t] > 0 else 0
+        conns.append((i, j, (int(p["yi"]), int(p["xi"])), (int(p["yj"]), int(p["xj"])), float(dist[idx_l[t]]),
+                      int(k_off[t]), conf, delta[t]))
         count[i] = count.get(i, 0) + 1
         count[j] = count.get(j, 0) + 1
     return conns
+
+
+def find_component_connections_fast(labeled_array, phase, components, conncomp_gap=None, max_neighbors=30,
+                                    n_neighbors=5, *, device='auto'):
+    """Same signature and result as utils_unwrap2d.find_component_connections_fast (:195-444).
+
+    labeled_array  int labels (0 = invalid); components: the reference's list of dicts ('label', 'size',
+    'slices'), in the order whose indices the connections use.  Returns
+    [(comp_i, comp_j, (row_i, col_i), (row_j, col_j), distance, k_offset, confidence, delta)].
+    """
+    torch = _torch()
+    n = len(components)
+    if n < 2:
+        return []
+    if n > 65535:
+        raise OverflowError("more than 65535 components")
+    labeled_array = np.asarray(labeled_array)
+    lut = np.zeros(int(labeled_array.max()) + 1, np.uint16)
+    for c, comp in enumerate(components):
+        lut[comp["label"]] = c + 1
+    lab16 = lut[labeled_array]
+    ph2 = np.asarray(phase, np.float32)
+    dev = resolve_device(device, None)
+    with torch.cuda.device(dev):
+        ph = torch.from_numpy(np.ascontiguousarray(ph2)).to(dev)
+        lab = torch.from_numpy(np.ascontiguousarray(lab16).view(np.int16)).to(dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _, _, pairs, npair, _ = _device_pairs(ph, lab, 1, int(max_neighbors), int(n_neighbors), dev, stream)
+    return _greedy_connections(pairs, npair, int(max_neighbors), conncomp_gap)
+
+
+def connect_components_ilp_fast(unwrapped, labeled_array, components, connections, max_time=60.0, debug=False):
+    """Same signature and result as utils_unwrap2d.connect_components_ilp_fast (:886-1040).
+
+    The integer program goes to the exact native solver (max_time is accepted and unused: the solve
+    is exact and fast); offsets reach only components connected to the first; float32 updates as the
+    reference's `result[labels == L] += k * 2 * np.pi`.
+    """
+    n = len(components)
+    if n < 2 or len(connections) == 0:
+        return unwrapped.copy()
+    sizes = [int(c["size"]) for c in components]
+    edges = _edge_weights(connections, sizes)
+    k = solve_offsets(n, edges)
+    k[~_reachable_from_first(n, edges)] = 0
+    result = unwrapped.copy()
+    labeled_array = np.asarray(labeled_array)
+    # a Python float added to the array: rounded to the array's dtype, added in that dtype
+    shift = np.zeros(int(labeled_array.max()) + 1, result.dtype)
+    for i, comp in enumerate(components):
+        if k[i] != 0:
+            shift[comp["label"]] = int(k[i]) * 2 * np.pi
+    add = shift[labeled_array]
+    moved = add != 0
+    result[moved] = result[moved] + add[moved]
+    if debug:
+        print(f"  Applied 2pi offsets to {int(np.count_nonzero(k))}/{n} components")
+    return result
 
 
 def unwrap2d(phase, weight=None, conncomp=False, conncomp_size=1000, conncomp_gap=None, conncomp_linksize=5,

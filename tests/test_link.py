@@ -225,6 +225,30 @@ def test_cuda_matches_reference_fixture(path):
     _check_cuda_vs(kw, d["connections"], d["out"])
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", GOLD, ids=IDS)
+def test_reference_signature_dropins_match_fixture(path):
+    """find_component_connections_fast / connect_components_ilp_fast with the reference's signatures,
+    driven through the _link_2d steps (Stack_unwrap2d.py:345-407)."""
+    _gpu()
+    from core_b200 import link as L
+    kw, d = load(path)
+    ph, cc = kw["phase"], kw["conncomp"]
+    min_size = max(kw["conncomp_size"], 4)
+    if cc is not None:
+        labeled, comps, sizes = O.components_from_labels(cc, min_size)
+    else:
+        labeled, comps, sizes = O.components_from_mask(~np.isnan(ph), min_size)
+    dicts = [{"label": lab, "size": sizes[lab], "slices": None} for lab in comps]
+    ph2 = ph.copy()
+    ph2[~(np.isin(labeled, comps) | (labeled == 0))] = np.nan
+    conns = L.find_component_connections_fast(labeled, ph2, dicts, kw["conncomp_gap"], kw["conncomp_linkcount"],
+                                              kw["conncomp_linksize"]) if len(comps) >= 2 else []
+    np.testing.assert_array_equal(conn_array(conns), d["connections"])
+    out = L.connect_components_ilp_fast(ph2, labeled, dicts, conns)
+    assert same_raster(out, d["out"])
+
+
 CASES = [
     # seed, H, W, blobs, holes, use labels, conncomp_size, gap, linksize, linkcount
     (101, 160, 200, 14, False, True, 30, None, 5, 30),
