@@ -38,7 +38,7 @@ struct Dinic {
     struct Arc { int to; Cap cap; };
     std::vector<Arc> arcs;
     std::vector<std::vector<int>> adj;
-    std::vector<int> level, it;
+    std::vector<int> level, it, path;
     explicit Dinic(int n) : adj(n), level(n), it(n) {}
     void add(int u, int v, Cap c) {
         if (c <= 0) return;
@@ -58,7 +58,7 @@ struct Dinic {
     }
     // one augmenting path in the level graph (explicit stack: paths can be long)
     Cap augment(int s, int t) {
-        std::vector<int> path;
+        path.clear();
         int u = s;
         while (true) {
             if (u == t) {
