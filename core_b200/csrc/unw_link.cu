@@ -437,61 +437,108 @@ __device__ __forceinline__ bool key_less(double da, int ja, double db, int jb) {
     return da < db || (da == db && ja < jb);
 }
 
+// Insert (d, j) into a thread's ascending list of at most K keys.
+__device__ __forceinline__ void topk_insert(double* md, int* mj, int& cnt, int K, double d, int j) {
+    if (cnt == K && !key_less(d, j, md[K - 1], mj[K - 1])) return;
+    int pos = cnt < K ? cnt++ : K - 1;
+    while (pos > 0 && key_less(d, j, md[pos - 1], mj[pos - 1])) {
+        md[pos] = md[pos - 1];
+        mj[pos] = mj[pos - 1];
+        pos--;
+    }
+    md[pos] = d;
+    mj[pos] = j;
+}
+
+// K rounds of a block-wide argmin over the heads of the per-thread lists:
+// res[r] = r-th smallest key's index (-1 past the end).  All threads call it.
+__device__ void topk_merge(const double* md, const int* mj, int cnt, int K, int* res, double* resd,
+                           double* bd, int* bj, int* bt) {
+    int head = 0;
+    for (int r = 0; r < K; r++) {
+        double d = head < cnt ? md[head] : INFINITY;
+        int j = head < cnt ? mj[head] : INT_MAX;
+        int t = threadIdx.x;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double od = __shfl_down_sync(FULL, d, o);
+            const int oj = __shfl_down_sync(FULL, j, o);
+            const int ot = __shfl_down_sync(FULL, t, o);
+            if (key_less(od, oj, d, j)) { d = od; j = oj; t = ot; }
+        }
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if (lane == 0) { bd[w] = d; bj[w] = j; bt[w] = t; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int k = 1; k < (int)(blockDim.x >> 5); k++)
+                if (key_less(bd[k], bj[k], bd[0], bj[0])) { bd[0] = bd[k]; bj[0] = bj[k]; bt[0] = bt[k]; }
+            res[r] = bj[0] == INT_MAX ? -1 : bj[0];
+            resd[r] = bd[0];
+        }
+        __syncthreads();
+        if (bj[0] != INT_MAX && bt[0] == (int)threadIdx.x) head++;
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ double bbox_dist(const LkComp& a, const LkComp& b) {
+    const long long dx = max(0, max(b.x0 - a.x1, a.x0 - b.x1));
+    const long long dy = max(0, max(b.y0 - a.y1, a.y0 - b.y1));
+    return sqrt((double)(dx * dx + dy * dy));
+}
+
 // One block per component in [c0, c1): the K nearest other components by
-// (hull distance, index); -1 pads.  Per-thread sorted lists, then a K-round merge.
+// (hull distance, index); -1 pads.  The bounding-box distance bounds the hull
+// distance from below, so: the K components nearest by that bound give exact
+// distances whose largest, T, bounds the K-th nearest from above; only
+// components with bound <= T need their exact distance.
 __global__ void k_lk_nbr(const LkComp* __restrict__ C, int n, int c0, int c1, const unsigned* __restrict__ hv, int K,
                          int* nbr) {
     extern __shared__ unsigned char smem[];
     double* sd = (double*)smem;
     int* sj = (int*)(sd + (size_t)blockDim.x * K);
-    __shared__ double bd[32];
-    __shared__ int bj[32], bt[32];
+    __shared__ double bd[32], resd[LK_MAX_K], thr;
+    __shared__ int bj[32], bt[32], res[LK_MAX_K];
     for (int i = c0 + blockIdx.x; i < c1; i += gridDim.x) {
         const LkComp Ci = C[i];
-        int* out = nbr + (size_t)(i - c0) * K;
         double* md = sd + (size_t)threadIdx.x * K;
         int* mj = sj + (size_t)threadIdx.x * K;
-        int cntl = 0;
-        if (Ci.hn >= 3) {
+        int cnt = 0;
+        const bool ok = Ci.hn >= 3;
+        // 1. the K nearest by the bounding-box bound
+        if (ok)
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                if (j == i || C[j].hn < 3) continue;
+                topk_insert(md, mj, cnt, K, bbox_dist(Ci, C[j]), j);
+            }
+        topk_merge(md, mj, cnt, K, res, resd, bd, bj, bt);
+        // 2. their exact distances: the threshold
+        // fewer than K others: no threshold; else the max of non-negative doubles, reduced
+        // as unsigned bit patterns from +0.0 (whose pattern is 0)
+        if (threadIdx.x == 0) thr = res[K - 1] < 0 ? INFINITY : 0.0;
+        __syncthreads();
+        double tmax = -INFINITY;
+        for (int r = threadIdx.x; r < K; r += blockDim.x) {
+            const int j = res[r];
+            if (j >= 0) tmax = fmax(tmax, hull_dist(hv + Ci.hoff, Ci.hn, hv + C[j].hoff, C[j].hn));
+        }
+        for (int o = 16; o > 0; o >>= 1) tmax = fmax(tmax, __shfl_down_sync(FULL, tmax, o));
+        if ((threadIdx.x & 31) == 0 && thr != INFINITY)
+            atomicMax((unsigned long long*)&thr, (unsigned long long)__double_as_longlong(fmax(tmax, 0.0)));
+        __syncthreads();
+        const double T = thr;
+        // 3. exact distances within the threshold
+        cnt = 0;
+        if (ok)
             for (int j = threadIdx.x; j < n; j += blockDim.x) {
                 if (j == i) continue;
                 const LkComp Cj = C[j];
-                if (Cj.hn < 3) continue;
-                const double d = hull_dist(hv + Ci.hoff, Ci.hn, hv + Cj.hoff, Cj.hn);
-                if (cntl == K && !key_less(d, j, md[K - 1], mj[K - 1])) continue;
-                int pos = cntl < K ? cntl++ : K - 1;
-                while (pos > 0 && key_less(d, j, md[pos - 1], mj[pos - 1])) {
-                    md[pos] = md[pos - 1];
-                    mj[pos] = mj[pos - 1];
-                    pos--;
-                }
-                md[pos] = d;
-                mj[pos] = j;
+                if (Cj.hn < 3 || bbox_dist(Ci, Cj) > T) continue;
+                topk_insert(md, mj, cnt, K, hull_dist(hv + Ci.hoff, Ci.hn, hv + Cj.hoff, Cj.hn), j);
             }
-        }
-        int head = 0;
-        for (int r = 0; r < K; r++) {
-            double d = head < cntl ? md[head] : INFINITY;
-            int j = head < cntl ? mj[head] : INT_MAX;
-            int t = threadIdx.x;
-            for (int o = 16; o > 0; o >>= 1) {
-                const double od = __shfl_down_sync(FULL, d, o);
-                const int oj = __shfl_down_sync(FULL, j, o);
-                const int ot = __shfl_down_sync(FULL, t, o);
-                if (key_less(od, oj, d, j)) { d = od; j = oj; t = ot; }
-            }
-            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-            if (lane == 0) { bd[w] = d; bj[w] = j; bt[w] = t; }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                for (int k = 1; k < (int)(blockDim.x >> 5); k++)
-                    if (key_less(bd[k], bj[k], bd[0], bj[0])) { bd[0] = bd[k]; bj[0] = bj[k]; bt[0] = bt[k]; }
-                out[r] = bj[0] == INT_MAX ? -1 : bj[0];
-            }
-            __syncthreads();
-            if (bj[0] != INT_MAX && bt[0] == (int)threadIdx.x) head++;
-            __syncthreads();
-        }
+        topk_merge(md, mj, cnt, K, res, resd, bd, bj, bt);
+        int* out = nbr + (size_t)(i - c0) * K;
+        for (int r = threadIdx.x; r < K; r += blockDim.x) out[r] = res[r];
+        __syncthreads();
     }
 }
 
