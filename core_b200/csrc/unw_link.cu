@@ -433,6 +433,33 @@ __device__ double hull_dist(const unsigned* P, int m, const unsigned* Q, int n) 
     return d;
 }
 
+// The same distance with the 32 lanes of a warp sharing the edge and vertex
+// loops (all lanes call it with the same arguments and get the same result).
+__device__ bool warp_separated(const unsigned* P, int m, const unsigned* Q, int n) {
+    bool found = false;
+    for (int k0 = 0; k0 < m && !found; k0 += 32) {
+        const int k = k0 + (threadIdx.x & 31);
+        bool all_out = k < m;
+        if (all_out) {
+            const unsigned a = P[k], b = P[k + 1 == m ? 0 : k + 1];
+            for (int q = 0; q < n && all_out; q++) all_out = crs_u(a, b, Q[q]) < 0;
+        }
+        found = __any_sync(FULL, all_out);
+    }
+    return found;
+}
+
+__device__ double warp_hull_dist(const unsigned* P, int m, const unsigned* Q, int n) {
+    if (!warp_separated(P, m, Q, n) && !warp_separated(Q, n, P, m)) return 0.0;
+    double d = INFINITY;
+    for (int i = threadIdx.x & 31; i < m; i += 32)
+        for (int k = 0; k < n; k++) d = fmin(d, pseg(P[i], Q[k], Q[k + 1 == n ? 0 : k + 1]));
+    for (int i = threadIdx.x & 31; i < n; i += 32)
+        for (int k = 0; k < m; k++) d = fmin(d, pseg(Q[i], P[k], P[k + 1 == m ? 0 : k + 1]));
+    for (int o = 16; o > 0; o >>= 1) d = fmin(d, __shfl_xor_sync(FULL, d, o));
+    return d;
+}
+
 __device__ __forceinline__ bool key_less(double da, int ja, double db, int jb) {
     return da < db || (da == db && ja < jb);
 }
@@ -511,29 +538,27 @@ __global__ void k_lk_nbr(const LkComp* __restrict__ C, int n, int c0, int c1, co
                 topk_insert(md, mj, cnt, K, bbox_dist(Ci, C[j]), j);
             }
         topk_merge(md, mj, cnt, K, res, resd, bd, bj, bt);
-        // 2. their exact distances: the threshold
-        // fewer than K others: no threshold; else the max of non-negative doubles, reduced
-        // as unsigned bit patterns from +0.0 (whose pattern is 0)
+        // 2. their exact distances (one warp per component): the threshold
         if (threadIdx.x == 0) thr = res[K - 1] < 0 ? INFINITY : 0.0;
         __syncthreads();
-        double tmax = -INFINITY;
-        for (int r = threadIdx.x; r < K; r += blockDim.x) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int r = warp; r < K; r += nw) {
             const int j = res[r];
-            if (j >= 0) tmax = fmax(tmax, hull_dist(hv + Ci.hoff, Ci.hn, hv + C[j].hoff, C[j].hn));
+            if (j < 0) continue;
+            const double d = warp_hull_dist(hv + Ci.hoff, Ci.hn, hv + C[j].hoff, C[j].hn);
+            if (lane == 0 && thr != INFINITY) atomicMax((unsigned long long*)&thr, (unsigned long long)__double_as_longlong(d));
         }
-        for (int o = 16; o > 0; o >>= 1) tmax = fmax(tmax, __shfl_down_sync(FULL, tmax, o));
-        if ((threadIdx.x & 31) == 0 && thr != INFINITY)
-            atomicMax((unsigned long long*)&thr, (unsigned long long)__double_as_longlong(fmax(tmax, 0.0)));
         __syncthreads();
         const double T = thr;
-        // 3. exact distances within the threshold
+        // 3. exact distances within the threshold, one warp per component, into lane 0's list
         cnt = 0;
         if (ok)
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            for (int j = warp; j < n; j += nw) {
                 if (j == i) continue;
                 const LkComp Cj = C[j];
                 if (Cj.hn < 3 || bbox_dist(Ci, Cj) > T) continue;
-                topk_insert(md, mj, cnt, K, hull_dist(hv + Ci.hoff, Ci.hn, hv + Cj.hoff, Cj.hn), j);
+                const double d = warp_hull_dist(hv + Ci.hoff, Ci.hn, hv + Cj.hoff, Cj.hn);
+                if (lane == 0) topk_insert(md, mj, cnt, K, d, j);
             }
         topk_merge(md, mj, cnt, K, res, resd, bd, bj, bt);
         int* out = nbr + (size_t)(i - c0) * K;

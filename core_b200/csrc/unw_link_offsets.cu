@@ -13,8 +13,9 @@
 // F is a global minimum.  The best move for each sign is a minimum cut: unit
 // moves change each pair term by a submodular table (the term is convex in the
 // difference), which is graph-representable (Kolmogorov & Zabih, 2004).  Cuts
-// are found with Dinic's max-flow in 128-bit integers (B * w * |d| exceeds
-// int64 for large instances); the moved set is the smallest
+// are found with Dinic's max-flow, in int64 when every finite capacity fits and
+// in 128-bit integers otherwise (B * w * |d| exceeds int64 for large
+// instances); the moved set is the smallest
 // minimiser (the nodes that still reach the sink in the residual graph), so the
 // result is deterministic.
 #include <stdint.h>
@@ -30,46 +31,60 @@
 
 namespace {
 
-using Cap = __int128;
-constexpr Cap CAP_MAX = (Cap)1 << 120;
-constexpr Cap HARD = (Cap)1 << 100;      // a forbidden move (outside the bounds)
+using Wide = __int128;
 
-struct Dinic {
-    struct Arc { int to; Cap cap; };
+// Dinic's max-flow on a graph built once per move: arcs in one array, the
+// arcs of a node contiguous (counted, then filled), an array queue.
+template <class Cap>
+struct Flow {
+    struct Arc { int to; int rev; Cap cap; };
+    int n = 0;
+    std::vector<int> start, level, it, queue, path;
     std::vector<Arc> arcs;
-    std::vector<std::vector<int>> adj;
-    std::vector<int> level, it, path;
-    explicit Dinic(int n) : adj(n), level(n), it(n) {}
+    std::vector<int> eu, ev;
+    std::vector<Cap> ec;
+    void reset(int nodes) { n = nodes; eu.clear(); ev.clear(); ec.clear(); }
     void add(int u, int v, Cap c) {
         if (c <= 0) return;
-        adj[u].push_back((int)arcs.size()); arcs.push_back({v, c});
-        adj[v].push_back((int)arcs.size()); arcs.push_back({u, 0});
+        eu.push_back(u); ev.push_back(v); ec.push_back(c);
+    }
+    void build() {
+        start.assign(n + 1, 0);
+        for (size_t e = 0; e < eu.size(); e++) { start[eu[e] + 1]++; start[ev[e] + 1]++; }
+        for (int v = 0; v < n; v++) start[v + 1] += start[v];
+        arcs.resize(start[n]);
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (size_t e = 0; e < eu.size(); e++) {
+            const int a = fill[eu[e]]++, b = fill[ev[e]]++;
+            arcs[a] = {ev[e], b, ec[e]};
+            arcs[b] = {eu[e], a, 0};
+        }
+        level.resize(n); it.resize(n); queue.resize(n);
     }
     bool bfs(int s, int t) {
         std::fill(level.begin(), level.end(), -1);
-        std::queue<int> q;
-        level[s] = 0; q.push(s);
-        while (!q.empty()) {
-            const int u = q.front(); q.pop();
-            for (int a : adj[u])
-                if (arcs[a].cap > 0 && level[arcs[a].to] < 0) { level[arcs[a].to] = level[u] + 1; q.push(arcs[a].to); }
+        int qh = 0, qt = 0;
+        level[s] = 0; queue[qt++] = s;
+        while (qh < qt) {
+            const int u = queue[qh++];
+            for (int a = start[u]; a < start[u + 1]; a++)
+                if (arcs[a].cap > 0 && level[arcs[a].to] < 0) { level[arcs[a].to] = level[u] + 1; queue[qt++] = arcs[a].to; }
         }
         return level[t] >= 0;
     }
     // one augmenting path in the level graph (explicit stack: paths can be long)
-    Cap augment(int s, int t) {
+    bool augment(int s, int t) {
         path.clear();
         int u = s;
         while (true) {
             if (u == t) {
-                Cap f = CAP_MAX;
+                Cap f = arcs[path[0]].cap;
                 for (int a : path) f = std::min(f, arcs[a].cap);
-                for (int a : path) { arcs[a].cap -= f; arcs[a ^ 1].cap += f; }
-                return f;
+                for (int a : path) { arcs[a].cap -= f; arcs[arcs[a].rev].cap += f; }
+                return true;
             }
             bool adv = false;
-            for (int& i = it[u]; i < (int)adj[u].size(); i++) {
-                const int a = adj[u][i];
+            for (int& a = it[u]; a < start[u + 1]; a++) {
                 if (arcs[a].cap > 0 && level[arcs[a].to] == level[u] + 1) {
                     path.push_back(a);
                     u = arcs[a].to;
@@ -78,81 +93,98 @@ struct Dinic {
                 }
             }
             if (!adv) {
-                if (path.empty()) return 0;
+                if (path.empty()) return false;
                 level[u] = -1;                      // dead end
                 const int a = path.back();
                 path.pop_back();
-                u = arcs[a ^ 1].to;
+                u = arcs[arcs[a].rev].to;
                 it[u]++;
             }
         }
     }
     void run(int s, int t) {
         while (bfs(s, t)) {
-            std::fill(it.begin(), it.end(), 0);
-            while (augment(s, t) > 0) {}
+            for (int v = 0; v < n; v++) it[v] = start[v];
+            while (augment(s, t)) {}
         }
     }
     // nodes that reach t in the residual graph (the smallest sink side)
     std::vector<char> reach_sink(int t) {
-        std::vector<char> r(adj.size(), 0);
-        std::vector<int> st{t};
-        r[t] = 1;
-        while (!st.empty()) {
-            const int v = st.back(); st.pop_back();
-            for (int a : adj[v]) {
-                const int u = arcs[a].to;          // arc a: v -> u; its pair a^1: u -> v
-                if (!r[u] && arcs[a ^ 1].cap > 0) { r[u] = 1; st.push_back(u); }
+        std::vector<char> r(n, 0);
+        int qt = 0;
+        r[t] = 1; queue[qt++] = t;
+        for (int qh = 0; qh < qt; qh++) {
+            const int v = queue[qh];
+            for (int a = start[v]; a < start[v + 1]; a++) {
+                const int u = arcs[a].to;          // arc v -> u; its reverse u -> v
+                if (!r[u] && arcs[arcs[a].rev].cap > 0) { r[u] = 1; queue[qt++] = u; }
             }
         }
         return r;
     }
 };
 
+constexpr Wide HARD = (Wide)1 << 100;      // a forbidden move (outside the bounds)
+constexpr int64_t HARD64 = (int64_t)1 << 62;
+
 struct Program {
     int n, m;
     const int32_t *ei, *ej, *off;
     const int64_t* w;
     int s;
-    Cap B;
-    Cap objective(const std::vector<int>& k) const {
-        Cap f = 0;
-        for (int e = 0; e < m; e++) f += B * (Cap)w[e] * (Cap)std::llabs((int64_t)s * (k[ei[e]] - k[ej[e]]) - off[e]);
+    Wide B;
+    bool narrow;                            // every finite capacity fits int64 with room
+    Flow<int64_t> f64;
+    Flow<Wide> f128;
+    Wide objective(const std::vector<int>& k) const {
+        Wide f = 0;
+        for (int e = 0; e < m; e++) f += B * (Wide)w[e] * (Wide)std::llabs((int64_t)s * (k[ei[e]] - k[ej[e]]) - off[e]);
         for (int i = 0; i < n; i++) f += std::llabs((int64_t)k[i]);
         return f;
     }
-    // the best set S for k + dir * chi_S (empty if none lowers F)
-    std::vector<char> best_move(const std::vector<int>& k, int dir) const {
+    // the smallest best set S for k + dir * chi_S (empty if no move lowers F)
+    template <class Cap>
+    std::vector<char> best_move(Flow<Cap>& g, const std::vector<int>& k, int dir, Cap hard) {
         const int S = n, T = n + 1;
-        Dinic g(n + 2);
-        std::vector<Cap> unary(n, 0);            // cost of x_v = 1 (moved) over x_v = 0
-        auto pair_term = [&](int u, int v, Cap A, Cap Bc, Cap Cc, Cap D) {
-            // E(x_u, x_v) = A + (C-A) x_u + (D-C) x_v + (B+C-A-D)(1-x_u) x_v
-            unary[u] += Cc - A;
-            unary[v] += D - Cc;
-            g.add(u, v, Bc + Cc - A - D);
-        };
+        g.reset(n + 2);
+        std::vector<Wide> unary(n, 0);           // cost of x_v = 1 (moved) over x_v = 0
         for (int e = 0; e < m; e++) {
             const int i = ei[e], j = ej[e];
             const int64_t d = (int64_t)s * (k[i] - k[j]) - off[e];
             const int64_t step = (int64_t)s * dir;       // change of d when only i moves
-            auto term = [&](int64_t dd) -> Cap { return std::llabs(dd) > 200 ? HARD : B * (Cap)w[e] * (Cap)std::llabs(dd); };
-            pair_term(i, j, term(d), term(d - step), term(d + step), term(d));
+            auto term = [&](int64_t dd) -> Wide { return std::llabs(dd) > 200 ? HARD : B * (Wide)w[e] * (Wide)std::llabs(dd); };
+            // E(x_i, x_j) = A + (C-A) x_i + (D-C) x_j + (B+C-A-D)(1-x_i) x_j
+            const Wide A = term(d), Bc = term(d - step), Cc = term(d + step), D = A;
+            unary[i] += Cc - A;
+            unary[j] += D - Cc;
+            g.add(i, j, (Cap)(Bc + Cc - A - D));
         }
         for (int v = 0; v < n; v++) {
             const int nk = k[v] + dir;
             if (v == 0 || nk < -100 || nk > 100) unary[v] += HARD;
-            else unary[v] += (Cap)(std::llabs((int64_t)nk) - std::llabs((int64_t)k[v]));
+            else unary[v] += (Wide)(std::llabs((int64_t)nk) - std::llabs((int64_t)k[v]));
         }
         for (int v = 0; v < n; v++) {
-            if (unary[v] > 0) g.add(S, v, unary[v]);    // paid when v is on the sink side (moved)
-            else if (unary[v] < 0) g.add(v, T, -unary[v]);
+            // paid when moved.  On the int64 path a forbidden node's unary is HARD plus a small
+            // term (no pair term is forbidden there), so it maps to the int64 HARD; the 128-bit
+            // path keeps exact values (its pair terms may carry +HARD / -HARD that must cancel)
+            if (unary[v] > 0) g.add(S, v, (sizeof(Cap) == 8 && unary[v] >= HARD / 2) ? hard : (Cap)unary[v]);
+            else if (unary[v] < 0) g.add(v, T, (Cap)(-unary[v]));
         }
+        g.build();
         g.run(S, T);
         std::vector<char> r = g.reach_sink(T);
-        std::vector<char> moved(n);
-        for (int v = 0; v < n; v++) moved[v] = r[v];
-        return moved;
+        r.resize(n);
+        return r;
+    }
+    std::vector<char> move(const std::vector<int>& k, int dir) {
+        // int64 is exact while no edge is at the +-200 bound (no forbidden pair terms) and
+        // every finite capacity fits (the caller checked the total)
+        bool edge_ok = true;
+        for (int e = 0; e < m && edge_ok; e++)
+            edge_ok = std::llabs((int64_t)s * (k[ei[e]] - k[ej[e]]) - off[e]) < 200;
+        if (narrow && edge_ok) return best_move<int64_t>(f64, k, dir, HARD64);
+        return best_move<Wide>(f128, k, dir, HARD);
     }
 };
 
@@ -215,20 +247,24 @@ extern "C" int unw_link_offsets(int32_t n, int32_t m, const int32_t* ei, const i
     if (n > (1 << 22)) return unw_set_error(UNW_E_UNSUPPORTED, "link offsets: too many components");
     std::vector<int> k(n, 0);
     if (n >= 2 && m > 0) {
-        Program P{n, m, ei, ej, off, w, sign >= 0 ? 1 : -1, (Cap)100 * n + 1};
+        Program P{n, m, ei, ej, off, w, sign >= 0 ? 1 : -1, (Wide)100 * n + 1, false, {}, {}};
+        Wide total = 0;                          // bound on the sum of finite capacities
+        for (int e = 0; e < m; e++) total += P.B * (Wide)w[e] * 4;
+        total += (Wide)4 * n;
+        P.narrow = total < ((Wide)1 << 60);
         k = spanning_start(P);
-        Cap f = P.objective(k);
+        Wide f = P.objective(k);
         for (int iter = 0; iter < 1000; iter++) {
-            Cap best = f;
+            Wide best = f;
             std::vector<int> kb;
             for (int dir = 1; dir >= -1; dir -= 2) {
-                const std::vector<char> S = P.best_move(k, dir);
+                const std::vector<char> S = P.move(k, dir);
                 std::vector<int> kn = k;
                 bool any = false;
                 for (int v = 0; v < n; v++)
                     if (S[v]) { kn[v] += dir; any = true; }
                 if (!any) continue;
-                const Cap fn = P.objective(kn);
+                const Wide fn = P.objective(kn);
                 if (fn < best) { best = fn; kb = kn; }
             }
             if (kb.empty()) break;
