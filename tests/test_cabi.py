@@ -95,3 +95,43 @@ def test_adjoint_rejects_bad_args_without_gpu():
     assert rc == _lib.UNW_E_ARG and "relative" in _lib.last_error()
     rc = call(f, 8, None, 8, 8, 8, C.byref(prm), f, 8, f, 8, f, 8, None, 8, f, 64, None, None)
     assert rc == _lib.UNW_E_WORKSPACE
+
+
+def test_link_entries_reject_bad_args_without_gpu():
+    lib = _lib.load()
+    assert lib.unw_link_workspace_bytes(4096, 4096, 1000) > 4096 * 4096 * 24
+    assert lib.unw_link_workspace_bytes(70000, 10, 4) == 0          # sides above 65535
+    assert C.sizeof(_lib.UnwLinkPair) == 64
+    f = C.c_void_p(0x10000)
+    prm = _lib.UnwLinkParams(30, 30, 5, 0)
+    n1, n2 = C.c_int32(0), C.c_int32(0)
+    rc = lib.unw_link_pairs_f32(None, 8, None, 8, 8, 8, C.byref(prm), None, None, None, 0, C.byref(n1), None, 0,
+                                C.byref(n2), f, 1 << 30, None)
+    assert rc == _lib.UNW_E_ARG
+    rc = lib.unw_link_pairs_f32(f, 4, None, 8, 8, 8, C.byref(prm), None, None, None, 0, C.byref(n1), None, 0,
+                                C.byref(n2), f, 1 << 30, None)
+    assert rc == _lib.UNW_E_ARG                                      # pitch below width
+    bad = _lib.UnwLinkParams(30, 30, 40, 0)                          # window above 31
+    rc = lib.unw_link_pairs_f32(f, 8, None, 8, 8, 8, C.byref(bad), None, None, None, 0, C.byref(n1), None, 0,
+                                C.byref(n2), f, 1 << 30, None)
+    assert rc == _lib.UNW_E_ARG
+    rc = lib.unw_link_pairs_f32(f, 8, None, 8, 8, 8, C.byref(prm), None, None, None, 0, C.byref(n1), None, 0,
+                                C.byref(n2), f, 16, None)
+    assert rc == _lib.UNW_E_WORKSPACE
+    k = (C.c_int32 * 2)(0, 1)
+    assert lib.unw_link_apply_f32(None, 8, 8, 8, k, 2, f, 8, f, 1 << 30, 30, None) == _lib.UNW_E_ARG
+    assert lib.unw_link_apply_f32(f, 8, 8, 8, k, 2, f, 8, f, 16, 30, None) == _lib.UNW_E_WORKSPACE
+
+
+def test_link_offsets_host_solver_without_gpu():
+    """unw_link_offsets is host code: it runs here.  Two components joined by one edge."""
+    lib = _lib.load()
+    ei, ej, off = (C.c_int32 * 1)(0), (C.c_int32 * 1)(1), (C.c_int32 * 1)(2)
+    w = (C.c_int64 * 1)(500)
+    k = (C.c_int32 * 2)()
+    assert lib.unw_link_offsets(2, 1, ei, ej, off, w, 1, k) == _lib.UNW_OK
+    assert list(k) == [0, -2]                    # k_0 - k_1 = 2 (reference sign)
+    assert lib.unw_link_offsets(2, 1, ei, ej, off, w, -1, k) == _lib.UNW_OK
+    assert list(k) == [0, 2]                     # k_1 - k_0 = 2
+    bad = (C.c_int32 * 1)(5)
+    assert lib.unw_link_offsets(2, 1, ei, bad, off, w, 1, k) == _lib.UNW_E_ARG
