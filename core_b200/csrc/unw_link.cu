@@ -604,15 +604,22 @@ __global__ void k_lk_pairs(const LkComp* __restrict__ C, const int2* __restrict_
         const LkComp T = swap ? Ci : Cj;
         if (threadIdx.x == 0) { best = ULLONG_MAX; key = ULLONG_MAX; blocked = 0; }
         __syncthreads();
-        // closest squared distance
+        // Closest pair with ties broken by (y_i, x_i, y_j, x_j).  The pruning is non-strict
+        // (a query or a row is skipped only when its bound exceeds the best squared distance),
+        // so every pair at the final minimum is seen: its query is not pruned, its row is within
+        // the bound, and its pixel is the nearest on its side of the row.
+        unsigned long long bd2 = ULLONG_MAX, bkey = ULLONG_MAX;
+        auto take = [&](unsigned long long d2, unsigned long long k2) {
+            if (d2 < bd2 || (d2 == bd2 && k2 < bkey)) { bd2 = d2; bkey = k2; }
+        };
         for (int q = threadIdx.x; q < S.nb; q += blockDim.x) {
             const unsigned pq = bpts[S.bstart + q];
             const int yq = py_(pq), xq = px_(pq);
-            unsigned long long loc = *(volatile unsigned long long*)&best;
-            if ((unsigned long long)bbox_d2(yq, xq, T) >= loc) continue;
+            unsigned long long loc = min(*(volatile unsigned long long*)&best, bd2);
+            if ((unsigned long long)bbox_d2(yq, xq, T) > loc) continue;
             const long long dy_lo = max(0LL, (long long)max(T.y0 - yq, yq - T.y1));
             for (long long dy = dy_lo;; dy++) {
-                if ((unsigned long long)(dy * dy) >= loc) break;
+                if ((unsigned long long)(dy * dy) > loc) break;
                 const bool up = yq - dy >= T.y0 && yq - dy <= T.y1;
                 const bool dn = dy > 0 && yq + dy >= T.y0 && yq + dy <= T.y1;
                 if (!up && !dn && (yq - dy < T.y0 && yq + dy > T.y1)) break;
@@ -624,50 +631,20 @@ __global__ void k_lk_pairs(const LkComp* __restrict__ C, const int2* __restrict_
                     const int k = lower_bound_u(bpts, lo, hi, pack_yx(y, xq));
                     if (k < hi) {
                         const long long dx = px_(bpts[k]) - xq;
-                        const unsigned long long d2 = (unsigned long long)(dx * dx + dy * dy);
-                        if (d2 < loc) loc = d2;
+                        take((unsigned long long)(dx * dx + dy * dy), pair_key(swap, yq, xq, y, px_(bpts[k])));
                     }
                     if (k > lo) {
                         const long long dx = xq - px_(bpts[k - 1]);
-                        const unsigned long long d2 = (unsigned long long)(dx * dx + dy * dy);
-                        if (d2 < loc) loc = d2;
+                        take((unsigned long long)(dx * dx + dy * dy), pair_key(swap, yq, xq, y, px_(bpts[k - 1])));
                     }
+                    loc = min(loc, bd2);
                 }
             }
-            atomicMin(&best, loc);
+            atomicMin(&best, bd2);
         }
         __syncthreads();
         const unsigned long long dmin = best;
-        // smallest (y_i, x_i, y_j, x_j) among the pairs at dmin
-        for (int q = threadIdx.x; q < S.nb; q += blockDim.x) {
-            const unsigned pq = bpts[S.bstart + q];
-            const int yq = py_(pq), xq = px_(pq);
-            if ((unsigned long long)bbox_d2(yq, xq, T) > dmin) continue;
-            const long long dy_lo = max(0LL, (long long)max(T.y0 - yq, yq - T.y1));
-            const long long dy_hi = max(yq - T.y0, T.y1 - yq);
-            for (long long dy = dy_lo; dy <= dy_hi && (unsigned long long)(dy * dy) <= dmin; dy++) {
-                const long long rem = (long long)dmin - dy * dy;
-                long long r = (long long)sqrt((double)rem);
-                while (r * r > rem) r--;
-                while ((r + 1) * (r + 1) <= rem) r++;
-                if (r * r != rem) continue;
-                for (int side = 0; side < 2; side++) {
-                    if (side == 1 && dy == 0) continue;
-                    const long long y = side == 0 ? yq - dy : yq + dy;
-                    if (y < T.y0 || y > T.y1) continue;
-                    const int s = T.rowoff + ((int)y - T.y0);
-                    const int lo = rstart[s], hi = rstart[s + 1];
-                    for (int sx = 0; sx < 2; sx++) {
-                        if (sx == 1 && r == 0) continue;
-                        const long long x = sx == 0 ? xq - r : xq + r;
-                        if (x < T.x0 || x > T.x1) continue;
-                        const unsigned want = pack_yx((int)y, (int)x);
-                        const int k = lower_bound_u(bpts, lo, hi, want);
-                        if (k < hi && bpts[k] == want) atomicMin(&key, pair_key(swap, yq, xq, (int)y, (int)x));
-                    }
-                }
-            }
-        }
+        if (bd2 == dmin) atomicMin(&key, bkey);
         __syncthreads();
         const unsigned long long kk = key;
         const unsigned pi = (unsigned)(kk >> 32), pj = (unsigned)kk;

@@ -24,6 +24,7 @@
 #include <climits>
 #include <cstdlib>
 #include <queue>
+#include <thread>
 #include <vector>
 
 #include "../../include/unwrap_b200.h"
@@ -134,8 +135,8 @@ struct Program {
     int s;
     Wide B;
     bool narrow;                            // every finite capacity fits int64 with room
-    Flow<int64_t> f64;
-    Flow<Wide> f128;
+    Flow<int64_t> f64[2];                   // one graph per move direction
+    Flow<Wide> f128[2];
     Wide objective(const std::vector<int>& k) const {
         Wide f = 0;
         for (int e = 0; e < m; e++) f += B * (Wide)w[e] * (Wide)std::llabs((int64_t)s * (k[ei[e]] - k[ej[e]]) - off[e]);
@@ -183,8 +184,9 @@ struct Program {
         bool edge_ok = true;
         for (int e = 0; e < m && edge_ok; e++)
             edge_ok = std::llabs((int64_t)s * (k[ei[e]] - k[ej[e]]) - off[e]) < 200;
-        if (narrow && edge_ok) return best_move<int64_t>(f64, k, dir, HARD64);
-        return best_move<Wide>(f128, k, dir, HARD);
+        const int slot = dir > 0 ? 0 : 1;
+        if (narrow && edge_ok) return best_move<int64_t>(f64[slot], k, dir, HARD64);
+        return best_move<Wide>(f128[slot], k, dir, HARD);
     }
 };
 
@@ -257,8 +259,13 @@ extern "C" int unw_link_offsets(int32_t n, int32_t m, const int32_t* ei, const i
         for (int iter = 0; iter < 1000; iter++) {
             Wide best = f;
             std::vector<int> kb;
+            // the two directions are independent cuts: the -1 move on a second thread
+            std::vector<char> Sdir[2];
+            std::thread down([&] { Sdir[1] = P.move(k, -1); });
+            Sdir[0] = P.move(k, 1);
+            down.join();
             for (int dir = 1; dir >= -1; dir -= 2) {
-                const std::vector<char> S = P.move(k, dir);
+                const std::vector<char>& S = Sdir[dir > 0 ? 0 : 1];
                 std::vector<int> kn = k;
                 bool any = false;
                 for (int v = 0; v < n; v++)

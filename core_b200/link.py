@@ -257,15 +257,15 @@ def _greedy_connections(pairs, npair, max_neighbors, gap):
     confidence = np.maximum(np.float32(0), np.float32(1.0) - np.float32(2) * np.abs(fractional))
     conns = []
     count = {}
-    ci_l, cj_l, idx_l, use_l = ci.tolist(), cj.tolist(), idx.tolist(), usable.tolist()
-    for t in range(len(idx_l)):
+    ci_l, cj_l, use_l = ci.tolist(), cj.tolist(), usable.tolist()
+    yi, xi, yj, xj = (P[f][idx].tolist() for f in ("yi", "xi", "yj", "xj"))
+    dl, kl = dist[idx].tolist(), np.where(usable, k_off, 0).astype(np.int64).tolist()
+    conf_l, delta_l, pos_l = list(confidence), list(delta), (confidence > 0).tolist()   # numpy float32 scalars
+    for t in range(len(ci_l)):
         i, j = ci_l[t], cj_l[t]
         if count.get(i, 0) >= max_neighbors or count.get(j, 0) >= max_neighbors or not use_l[t]:
             continue
-        p = P[idx_l[t]]
-        conf = confidence[t] if confidence[t] > 0 else 0
-        conns.append((i, j, (int(p["yi"]), int(p["xi"])), (int(p["yj"]), int(p["xj"])), float(dist[idx_l[t]]),
-                      int(k_off[t]), conf, delta[t]))
+        conns.append((i, j, (yi[t], xi[t]), (yj[t], xj[t]), dl[t], kl[t], conf_l[t] if pos_l[t] else 0, delta_l[t]))
         count[i] = count.get(i, 0) + 1
         count[j] = count.get(j, 0) + 1
     return conns
