@@ -185,7 +185,11 @@ def link_components(phase, conncomp=None, conncomp_size=100, conncomp_gap=None, 
         if is_torch and phase.is_cuda:
             res = out_t
         else:
-            res = out_t.cpu().numpy() if not is_torch else out_t.cpu()
+            # through a pinned host block (torch's host caching allocator recycles it)
+            host = torch.empty(out_t.shape, dtype=out_t.dtype, pin_memory=True)
+            host.copy_(out_t, non_blocking=True)
+            torch.cuda.current_stream(out_t.device).synchronize()
+            res = host if is_torch else host.numpy()
         if squeeze:
             res = res[None]
         return (res, info) if return_info else res
