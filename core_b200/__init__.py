@@ -9,7 +9,7 @@ from .irls import irls_unwrap_2d, irls_unwrap_2d_batch, resolve_device  # noqa: 
 from .adapters import unwrap2d_chunk  # noqa: F401
 from .autodiff import irls_adjoint, irls_unwrap_2d_diff  # noqa: F401
 from .goldstein import goldstein  # noqa: F401
-from .link import link_components, unwrap2d  # noqa: F401
+from .link import link_components, unwrap2d, unwrap2d_link  # noqa: F401
 
 __all__ = ["irls_unwrap_2d", "irls_unwrap_2d_batch", "unwrap2d_chunk", "irls_unwrap_2d_diff", "irls_adjoint",
-           "goldstein", "link_components", "unwrap2d"]
+           "goldstein", "link_components", "unwrap2d", "unwrap2d_link"]

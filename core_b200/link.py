@@ -333,6 +333,23 @@ def connect_components_ilp_fast(unwrapped, labeled_array, components, connection
     return result
 
 
+def unwrap2d_link(phase, conncomp_size=10_000, conncomp_gap=None, conncomp_linksize=5, conncomp_linkcount=30,
+                  debug=False, *, device='auto'):
+    """Stack.unwrap2d_link (Stack_unwrap2d.py:460-523) on numpy / torch arrays: link the components of
+    already unwrapped phase, labels from the valid mask.  phase (H, W) or (n, H, W)."""
+    if conncomp_linksize > conncomp_size:
+        raise ValueError(
+            f'conncomp_linksize ({conncomp_linksize}) cannot be greater than conncomp_size ({conncomp_size}). '
+            f'Components must have at least conncomp_linksize pixels for reliable offset estimation.')
+    kw = dict(conncomp_size=conncomp_size, conncomp_gap=conncomp_gap, conncomp_linksize=conncomp_linksize,
+              conncomp_linkcount=conncomp_linkcount, debug=debug, device=device)
+    if phase.ndim == 2:
+        return link_components(phase, None, **kw)
+    torch = _torch()
+    outs = [link_components(phase[i], None, **kw) for i in range(phase.shape[0])]
+    return torch.stack(outs) if isinstance(phase, torch.Tensor) else np.stack(outs)
+
+
 def unwrap2d(phase, weight=None, conncomp=False, conncomp_size=1000, conncomp_gap=None, conncomp_linksize=5,
              conncomp_linkcount=30, device='auto', debug=False, **kwargs):
     """IRLS unwrap then component linking (Stack.unwrap2d, Stack_unwrap2d.py:525-640), on numpy / torch arrays.

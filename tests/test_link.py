@@ -343,3 +343,77 @@ def test_cuda_large_grid_properties():
     assert info["k"][0] == 0
     small = (cc > 0) & ~np.isin(cc, comps)
     assert np.isnan(out[small]).all()
+
+
+EDGE = [
+    # name, kwargs for the scene and link, transformed labels
+    ("window0", dict(conncomp_linksize=0), None),
+    ("window1", dict(conncomp_linksize=1), None),
+    ("window31", dict(conncomp_linksize=31), None),
+    ("k_all", dict(conncomp_linkcount=1000), None),
+    ("k0", dict(conncomp_linkcount=0), None),
+    ("gap0", dict(conncomp_gap=0.0), None),
+    ("label_gaps", dict(), "gaps"),
+    ("edges", dict(), "edges"),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,kw,mode", EDGE, ids=[e[0] for e in EDGE])
+def test_cuda_edge_parameters_match_oracle(name, kw, mode):
+    _gpu()
+    import core_b200
+    ph, cc = _scene(111, 140, 190, 16, True)
+    if mode == "gaps":                      # label values with holes in the numbering
+        cc = np.where(cc > 0, cc * 3 + 7, 0).astype(np.uint16)
+    if mode == "edges":                     # components cut by every raster edge
+        ph, cc = ph[20:120, 30:160].copy(), cc[20:120, 30:160].copy()
+        from scipy import ndimage
+        lab, n = ndimage.label(cc > 0, structure=O.STRUCT4)
+        sizes = np.bincount(lab.ravel(), minlength=n + 1)
+        order = sorted(range(1, n + 1), key=lambda L: (-sizes[L], -L))
+        lut = np.zeros(n + 1, np.uint16)
+        lut[order] = np.arange(1, n + 1)
+        cc = lut[lab]
+        ph[cc == 0] = np.nan
+    args = dict(conncomp_size=20)
+    args.update(kw)
+    for labels in (cc, None):
+        ref, rinfo = O.link(ph, labels, return_info=True, **args)
+        out, info = core_b200.link_components(ph, labels, return_info=True, **args)
+        np.testing.assert_array_equal(conn_array(info["connections"]), conn_array(rinfo["connections"]))
+        assert same_raster(out, ref)
+
+
+@pytest.mark.gpu
+def test_unwrap2d_link_stack_and_validation():
+    _gpu()
+    import core_b200
+    a, _ = _scene(112, 120, 150, 12, False)
+    b, _ = _scene(113, 120, 150, 12, True)
+    out = core_b200.unwrap2d_link(np.stack([a, b]), conncomp_size=40)
+    for k, ph in enumerate((a, b)):
+        assert same_raster(out[k], O.link(ph, None, conncomp_size=40))
+    with pytest.raises(ValueError):
+        core_b200.unwrap2d_link(a, conncomp_size=4, conncomp_linksize=5)
+
+
+@pytest.mark.gpu
+def test_cuda_lines_only_and_single_component():
+    """Straight-line components take no part (no contour polygon); one component: NaN filter only."""
+    _gpu()
+    import core_b200
+    ph = np.full((40, 60), np.nan, np.float32)
+    ph[5, 2:50] = 1.0
+    ph[20, 3:58] = 2.0
+    ph[30:39, 10] = 3.0
+    for labels in (None,):
+        out, info = core_b200.link_components(ph, labels, conncomp_size=5, return_info=True)
+        assert len(info["components"]) == 3 and info["connections"] == []
+        assert same_raster(out, ph)
+    blob = np.full((30, 30), np.nan, np.float32)
+    blob[5:20, 5:20] = 0.5
+    blob[25, 25] = 9.0                      # a one-pixel component below the size: NaN
+    out = core_b200.link_components(blob, conncomp_size=10)
+    ref = O.link(blob, conncomp_size=10)
+    assert same_raster(out, ref) and np.isnan(out[25, 25])
