@@ -61,6 +61,7 @@ constexpr int MAX_GEN = 28672;
 constexpr int NUM_SMS = 148;
 constexpr int CTAS_ROW = NUM_SMS * 4;
 constexpr int CTAS_MATVEC = NUM_SMS * 2;
+constexpr int CTAS_HEAD = NUM_SMS * 4;
 
 size_t up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -305,7 +306,7 @@ int kind_ctas(const GridDev& G, int kind) {
         // persistent kinds: at most a few CTAs per SM, each loops over its units
         case KS_ROWPAIR: return std::min((G.H + 1) / 2, CTAS_ROW);
         case KS_COL: return std::min((G.W + 2 * G.col_nseq - 1) / (2 * G.col_nseq), G.col_ctas);
-        case KS_STEN: return G.sten_tiles_x * ((G.H + 8 * G.sten_rows - 1) / (8 * G.sten_rows));
+        case KS_STEN: return std::min(G.sten_tiles_x * ((G.H + 8 * G.sten_rows - 1) / (8 * G.sten_rows)), CTAS_HEAD);
         case KS_MATVEC: return std::min(G.sten_tiles_x * ((G.H + 15) / 16), CTAS_MATVEC);
         case KS_ELEM: return elem_ctas(npx);
         case KS_ONE: return 1;

@@ -449,8 +449,10 @@ __device__ __forceinline__ float irls_w(float w, float r, float eps2) {
     return clampf_nan(fdiv(w, __fsqrt_rn(fadd(fmul(r, r), eps2))), 1e-6f, 1e6f);
 }
 
-__global__ void __launch_bounds__(256) k_head(const GridDev* __restrict__ grids,
-                                              const int* __restrict__ starts, int n, int it) {
+// Persistent: a CTA loops over 128 x 8 tiles and arrives once with its partial
+// sums (one block reduction and one atomic per CTA, not per tile).
+__global__ void __launch_bounds__(256, 4) k_head(const GridDev* __restrict__ grids,
+                                                 const int* __restrict__ starts, int n, int it) {
     __shared__ double red[32 * 2];
     const int g = find_grid(starts, n, blockIdx.x);
     const GridDev& G = grids[g];
@@ -460,14 +462,16 @@ __global__ void __launch_bounds__(256) k_head(const GridDev* __restrict__ grids,
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tx = local % G.sten_tiles_x, ty = local / G.sten_tiles_x;
-    const int j0 = tx * 128 + lane * 4;
-    const int i = ty * 8 + warp;
     const float m = st->vcount > 0 ? (float)st->mean : 0.f;
     const float eps2 = st->eps2;
     const float* __restrict__ uc = (it & 1) ? G.U1 : G.U0;
     float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
     double acc[2] = {0.0, 0.0};
+    const int ntiles = G.sten_tiles_x * ((H + 8 * G.sten_rows - 1) / (8 * G.sten_rows));
+    for (int tile = local; tile < ntiles; tile += nct) {
+    const int tx = tile % G.sten_tiles_x, ty = tile / G.sten_tiles_x;
+    const int j0 = tx * 128 + lane * 4;
+    const int i = ty * 8 + warp;
     const bool on = i < H && j0 < W;
     const bool hu = i > 0, hd = i < H - 1;
     const size_t o = (size_t)i * P + j0;
@@ -533,6 +537,7 @@ __global__ void __launch_bounds__(256) k_head(const GridDev* __restrict__ grids,
         st4(G.wIx, o, wix);
         st4(G.wIy, o, wiy);
         st4(G.b, o, bv);
+    }
     }
     if (arrive<2>(G, local, nct, acc, red)) {
         finish_sum<2>(G, nct, acc, red);
