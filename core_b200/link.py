@@ -108,7 +108,7 @@ def _device_labels(conncomp, dev, H, W):
                 raise ValueError("conncomp labels must lie in [0, 65535]")
             t = t.to(torch.int32).to(torch.int16) if int(t.max()) < 32768 else \
                 torch.from_numpy(t.cpu().numpy().astype(np.uint16).view(np.int16))
-        t = t.to(dev).contiguous()
+        t = t.to(dev, non_blocking=t.device.type == "cpu" and t.is_pinned()).contiguous()
     else:
         a = np.asarray(conncomp)
         if a.dtype != np.uint16:
@@ -196,7 +196,8 @@ def link_components(phase, conncomp=None, conncomp_size=100, conncomp_gap=None, 
 
     with torch.cuda.device(dev):
         if is_torch:
-            ph = ph2.to(device=dev, dtype=torch.float32).contiguous()
+            ph = ph2.to(device=dev, dtype=torch.float32,
+                        non_blocking=ph2.device.type == "cpu" and ph2.is_pinned()).contiguous()
         else:
             ph = torch.from_numpy(np.ascontiguousarray(ph2, dtype=np.float32)).to(dev)
         if bool(torch.isnan(ph).all()):
