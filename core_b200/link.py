@@ -129,7 +129,9 @@ def _device_pairs(ph, lab, min_size, K, window, dev, stream):
     ws = _ws().get(dev, lib.unw_link_workspace_bytes(H, W, min_size))
     ncomp, npair = C.c_int32(0), C.c_int32(0)
     ccap, pcap = 1024, 1024 * max(K, 1)
-    for _ in range(2):
+    # A call that finds its output arrays too small reports the counts it reached: first the
+    # components, then (on the next call) the candidate pairs, so at most three calls.
+    for attempt in range(3):
         clab = np.zeros(ccap, np.int64)
         csz = np.zeros(ccap, np.int64)
         cfl = np.zeros(ccap, np.int32)
@@ -137,12 +139,16 @@ def _device_pairs(ph, lab, min_size, K, window, dev, stream):
         rc = lib.unw_link_pairs_f32(ph.data_ptr(), W, lab.data_ptr() if lab is not None else None, W, H, W,
                                     C.byref(prm), clab.ctypes.data, csz.ctypes.data, cfl.ctypes.data, ccap,
                                     C.byref(ncomp), pairs, pcap, C.byref(npair), ws.data_ptr(), ws.numel(), stream)
-        if rc == _lib.UNW_E_WORKSPACE and (ncomp.value > ccap or npair.value > pcap):
-            ccap, pcap = max(ccap, ncomp.value), max(pcap, npair.value)
+        if rc == _lib.UNW_E_WORKSPACE and (ncomp.value > ccap or npair.value > pcap) and attempt < 2:
+            # each component adds at most K candidate pairs: size for that (bounded) once n is known
+            bound = min(ncomp.value * max(K, 1), 1 << 24)
+            ccap, pcap = max(ccap, ncomp.value), max(pcap, npair.value, bound)
             continue
         _lib.check(rc, "unw_link_pairs_f32")
         break
     n = ncomp.value
+    if n > len(clab) or npair.value > len(pairs):
+        raise RuntimeError("unw_link_pairs_f32: output arrays not filled")
     return clab[:n].copy(), csz[:n].copy(), pairs, npair.value, ws
 
 

@@ -417,3 +417,48 @@ def test_cuda_lines_only_and_single_component():
     out = core_b200.link_components(blob, conncomp_size=10)
     ref = O.link(blob, conncomp_size=10)
     assert same_raster(out, ref) and np.isnan(out[25, 25])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prob,K", [(0.5, 30), (0.4, 30), (0.5, 3), (0.6, 5)])
+def test_cuda_noisy_mask_matches_oracle(prob, K):
+    """Dense random masks: many small interleaved components, most hulls overlapping."""
+    _gpu()
+    import core_b200
+    rng = np.random.default_rng(int(prob * 100) + K)
+    valid = rng.random((60, 80)) < prob
+    ph = np.where(valid, rng.normal(0, 1, (60, 80)), np.nan).astype(np.float32)
+    ref, rinfo = O.link(ph, None, conncomp_size=4, conncomp_linkcount=K, return_info=True)
+    out, info = core_b200.link_components(ph, None, conncomp_size=4, conncomp_linkcount=K, return_info=True)
+    assert len(info["components"]) == len(rinfo["components"])
+    np.testing.assert_array_equal(conn_array(info["connections"]), conn_array(rinfo["connections"]))
+    assert same_raster(out, ref)
+
+
+@pytest.mark.gpu
+def test_cuda_many_components_fill_the_pair_arrays():
+    """Thousands of components: more components and candidate pairs than the first output arrays
+    hold, so the host call is repeated with larger arrays; the 4-connected components and the
+    candidate pairs must come back complete (checked on a sample against the oracle's geometry)."""
+    _gpu()
+    import core_b200
+    from core_b200 import link as L
+    import torch
+    rng = np.random.default_rng(3)
+    valid = rng.random((512, 512)) < 0.5
+    ph = np.where(valid, rng.normal(0, 1, (512, 512)), np.nan).astype(np.float32)
+    dev = torch.device("cuda", 0)
+    t = torch.from_numpy(ph).to(dev)
+    clab, csz, pairs, npair, _ = L._device_pairs(t, None, 4, 30, 5, dev, torch.cuda.current_stream(dev).cuda_stream)
+    labeled, comps, sizes = O.components_from_mask(valid, 4)
+    assert len(clab) == len(comps) > 1024
+    assert list(csz) == [int(sizes[c]) for c in comps]
+    P = np.ctypeslib.as_array(pairs, shape=(len(pairs),))[:npair]
+    assert npair > 1024 * 30 and (P["comp_i"] < P["comp_j"]).all() and (P["d2"] > 0).all()
+    for k in rng.choice(npair, 40, replace=False):
+        i, j = int(P["comp_i"][k]), int(P["comp_j"][k])
+        d2, yi, xi, yj, xj = O.nearest_pair(O.border_points(labeled, comps[i]), O.border_points(labeled, comps[j]))
+        assert (int(P["d2"][k]), int(P["yi"][k]), int(P["xi"][k]), int(P["yj"][k]), int(P["xj"][k])) == \
+            (d2, yi, xi, yj, xj)
+    out, info = core_b200.link_components(ph, None, conncomp_size=4, return_info=True)
+    assert len(info["connections"]) > 0
