@@ -176,6 +176,8 @@ def link_components(phase, conncomp=None, conncomp_size=100, conncomp_gap=None, 
     torch = _torch()
     if sign not in ("reference", "aligned"):
         raise ValueError("sign must be 'reference' or 'aligned'")
+    if not 0 <= int(conncomp_linksize) <= 31:
+        raise ValueError("conncomp_linksize must lie in [0, 31] (windows of at most 31 x 31 pixels)")
     is_torch = isinstance(phase, torch.Tensor)
     squeeze = phase.ndim == 3 and phase.shape[0] == 1
     ph2 = phase[0] if squeeze else phase
@@ -372,6 +374,11 @@ def unwrap2d(phase, weight=None, conncomp=False, conncomp_size=1000, conncomp_ga
             f'Components must have at least conncomp_linksize pixels for reliable offset estimation.')
     kw = dict(max_iter=50, tol=1e-2, cg_max_iter=10, cg_tol=1e-3, epsilon=1e-2)
     kw.update(kwargs)
+    torch = _torch()
+    if isinstance(phase, torch.Tensor):
+        phase = phase.detach().cpu().numpy()
+    if isinstance(weight, torch.Tensor):
+        weight = weight.detach().cpu().numpy()
     a = np.asarray(phase, np.float32)
     single = a.ndim == 2
     stack = a[None] if single else a
