@@ -375,7 +375,11 @@ __global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ g
     double acc[1] = {0.0};
     const int ntiles = G.sten_tiles_x * ((H + 15) / 16);
     for (int tile = local; tile < ntiles; tile += nct) {
-    const int tx = tile % G.sten_tiles_x, ty = tile / G.sten_tiles_x;
+    // bottom rows first: the row-inverse pass that formed p ends at the bottom, so
+    // its last rows are still in L2, and the row-forward pass that reads Ap next
+    // starts at the top, where this pass ends
+    const int tr = ntiles - 1 - tile;
+    const int tx = tr % G.sten_tiles_x, ty = tr / G.sten_tiles_x;
     const int j0 = tx * 128 + lane * 4;
     const int i = ty * 16 + warp;
     // lanes past the last column load nothing (j0 < W implies j0 + 3 < P)

@@ -172,10 +172,13 @@ def main():
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--large", action="store_true", help="also the 1024^2 grids")
     ap.add_argument("--xlarge", action="store_true", help="also the 4096^2 fault grid (~8 min)")
+    ap.add_argument("--xlarge64", action="store_true",
+                    help="FP64 runs at full size: the 4096^2 fault grid and the G1 grid at 2048^2 and 4096^2")
     ap.add_argument("--only", default=None)
+    ap.add_argument("--no-small", action="store_true", help="skip the small fixtures")
     a = ap.parse_args()
     f32, f64 = load_reference(a.ref)
-    if not (a.only and a.only.startswith("L")):
+    if not (a.no_small or (a.only and a.only.startswith("L"))):
         for name, p, c, params in cases_small():
             if a.only and a.only != name:
                 continue
@@ -200,6 +203,16 @@ def main():
         u, cc, it, s = run_ref(f32, p, c, FN_DEFAULTS)
         save_large("L_g2_4096_fn_fp32", "g2", (4096, 4096, 0), FN_DEFAULTS, p, u, cc, it, s, "fp32", 16)
         print(f"L_g2_4096_fn_fp32: iters={it} {s:.2f}s")
+    if a.xlarge64:
+        for name, gen, args, step in (("L_g1_2048_fn_fp64", "g1", (2048, 2048, 0), 8),
+                                      ("L_g2_4096_fn_fp64", "g2", (4096, 4096, 0), 16),
+                                      ("L_g1_4096_fn_fp64", "g1", (4096, 4096, 0), 16)):
+            if a.only and a.only != name:
+                continue
+            p, c, _ = gen_g1(args[0], args[1], seed=args[2]) if gen == "g1" else gen_g2(args[0], seed=args[2])
+            u, cc, it, s = run_ref(f64, p, c, FN_DEFAULTS)
+            save_large(name, gen, args, FN_DEFAULTS, p, u, cc, it, s, "fp64", step)
+            print(f"{name}: iters={it} {s:.2f}s", flush=True)
 
 
 if __name__ == "__main__":
