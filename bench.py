@@ -18,7 +18,9 @@ Printed JSON (rank 0, one line):
   roofline   dominant kernel's algorithmic bytes / its mean CUDA-event launch
              time inside the timed region, against MEASURED_PEAKS.json hbm_gbs;
   cpu_baseline  the numpy oracle on the GPU host's cores, bounded sample;
-  clocks     nvidia-smi samples taken during the timed region.
+  clocks     nvidia-smi samples taken during the timed region;
+  accuracy   cycle-map match and RMS of the output against the reference's own
+             FP64 and FP32 runs of the bench grid (committed fixtures).
 """
 from __future__ import annotations
 
@@ -301,6 +303,10 @@ def run_b200(args):
     t_e2e = barrier_max(t_e2e, world, local)
     e2e = world * npx * e2e_steps / 1e6 / t_e2e
 
+    # ---- accuracy of this run's output against the reference's own runs of the same grid
+    # (committed fixtures: full 2-pi cycle map + unwrapped phase on a sub-sampled lattice)
+    accuracy = accuracy_vs_reference(p, u_np) if (rank == 0 and args.shape is None) else None
+
     # ---- roofline of the dominant kernel (live event times from the timed region)
     names = _lib.PROF_NAMES
     peak, peak_kind = load_peaks()
@@ -385,13 +391,38 @@ def run_b200(args):
            "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(npx * 8),
                    "d2h_bytes_per_step": int(npx * 6)},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches // 1,
-           "stack": stack, "link": link}
+           "stack": stack, "link": link, "accuracy": accuracy}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def accuracy_vs_reference(p, u):
+    """Cycle-map match and RMS (after mean removal, on the fixture's lattice) of the
+    4096^2 fault-grid output against the reference function's FP64 and FP32 runs of
+    the same input (tests/golden/L_g2_4096_fn_fp64.npz, L_g2_4096_fn_fp32.npz)."""
+    out = {}
+    v = np.isfinite(p)
+    k = np.zeros(p.shape, np.int16)
+    k[v] = np.round((u[v].astype(np.float64) - p[v].astype(np.float64)) / (2 * np.pi)).astype(np.int16)
+    for prec in ("fp64", "fp32"):
+        f = os.path.join(REPO, "tests", "golden", f"L_g2_4096_fn_{prec}.npz")
+        if not os.path.exists(f):
+            continue
+        d = np.load(f)
+        if tuple(d["cycles"].shape) != p.shape:
+            continue
+        s = int(d["step"])
+        vs = v[::s, ::s]
+        e = (u[::s, ::s].astype(np.float64) - d["u_sub"].astype(np.float64))[vs]
+        out[f"vs_reference_{prec}"] = {
+            "cycle_match": round(float((k == d["cycles"])[v].mean()), 6),
+            "rms_rad": float(f"{np.sqrt(np.mean((e - e.mean()) ** 2)):.3g}"),
+            "lattice": f"every {s}th row and column ({int(vs.sum())} valid pixels)"}
+    return out or None
 
 
 # --------------------------------------------------------------------------- stack workload
