@@ -13,8 +13,8 @@ max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2):
 Printed JSON (rank 0, one line):
   value      Mpx/s with inputs resident in HBM (C ABI on device pointers),
              K solves timed with CUDA events, max over ranks, barrier both sides;
-  e2e        same metric through the public API irls_unwrap_2d with pinned host
-             input and numpy output (H2D + D2H inside the timed region);
+  e2e        same metric through the public API irls_unwrap_2d with numpy input
+             and numpy output (H2D + D2H inside the timed region);
   roofline   dominant kernel's algorithmic bytes / its mean CUDA-event launch
              time inside the timed region, against MEASURED_PEAKS.json hbm_gbs;
   cpu_baseline  the numpy oracle on the GPU host's cores, bounded sample;
@@ -177,15 +177,47 @@ def cpu_sample(p, c, n_irls, workers):
     return t0, t1, full
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_irls_count(p, c, shape, workers):
+    """IRLS iterations of the full solve of this workload: the reference function's own
+    float32 run of the 4096^2 fault grid (stored with its cycle map in
+    tests/golden/L_g2_4096_fn_fp32.npz); for other shapes, one full oracle solve."""
+    if shape is None:
+        f = os.path.join(REPO, "tests", "golden", "L_g2_4096_fn_fp32.npz")
+        if os.path.exists(f):
+            return int(np.load(f)["iters"]), "the reference function's own float32 run of this grid"
+    from oracle.irls_oracle import OracleStats, irls_unwrap_2d as oracle
+    st = OracleStats()
+    oracle(p, c, workers=workers, stats=st, **FN)
+    return int(st.irls_iters), "a full oracle solve of this grid"
+
+
 def run_reference(args):
-    """--impl reference: the oracle restatement of the reference's CPU path."""
+    """--impl reference: the reference's CPU path, restated by the oracle, on the host cores.
+
+    One step = one IRLS iteration (20 PCG iterations, the same array work as every IRLS
+    iteration of the full solve) of the workload's solve, timed on the host clock; the
+    setup + DCT initial solve + post-processing is timed once beforehand.  `ms_per_step`
+    is that measured step time.  `value` is in the GPU arm's unit, Mpx of full solves per
+    second: grid pixels / (setup-and-post time + IRLS count x median step time), the IRLS
+    count being that of the reference's own run of the same grid."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    import scipy.fft
     workers = os.cpu_count()
     p, c = make_input(shape=args.shape)
     npx = p.size
-    n_irls = 30  # IRLS iterations of this solve under function defaults (reference CPU run)
+    n_irls, n_src = reference_irls_count(p, c, args.shape, workers)
     from oracle.irls_oracle import irls_unwrap_2d as oracle
     t = time.perf_counter()
     oracle(p, c, workers=workers, **dict(FN, max_iter=0))
@@ -200,16 +232,31 @@ def run_reference(args):
     t_irls = float(np.median(samples))
     full = t0 + n_irls * t_irls
     value = npx / 1e6 / full
-    sample = (f"per step: 1 IRLS iteration (20 PCG) of the 4096^2 solve; full solve = "
-              f"init+post {t0:.1f}s + {n_irls} x {t_irls:.1f}s")
+    sample = (f"per step: one IRLS iteration (20 PCG) of the {p.shape[0]}x{p.shape[1]} solve, measured "
+              f"{t_irls:.2f} s (median of {args.steps}); setup + DCT init + post measured once {t0:.2f} s; "
+              f"full solve = {t0:.1f} + {n_irls} x {t_irls:.2f} = {full:.0f} s, {n_irls} IRLS iterations "
+              f"from {n_src}")
+    cpu = {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample,
+           "cpu_model": cpu_model(), "os_cpu_count": os.cpu_count(), "scipy_fft_workers": workers,
+           "numpy_threads_note": "the oracle's FFTs run on scipy.fft with workers=cores; its elementwise "
+                                 "numpy work is single-threaded"}
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": full * 1e3, "higher_is_better": True, "scaling": "weak",
+           "warmup": args.warmup, "ms_per_step": t_irls * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-           "config": {"workload": workload_name(args.shape), "grid": list(p.shape), "params": FN},
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
+           "config": workload_config(p.shape, args.shape, args.gpus),
+           "full_solve_s_extrapolated": full, "irls_iters_full_solve": n_irls,
+           "step_definition": "one IRLS iteration of the full solve (ms_per_step is measured; value "
+                              "extrapolates to the full solve)",
+           "cpu_baseline": cpu,
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
+
+
+def workload_config(grid_shape, shape_arg, n_gpus):
+    """The `config` both arms print (identical for the same workload)."""
+    return {"workload": workload_name(shape_arg), "grid": [int(grid_shape[0]), int(grid_shape[1])],
+            "params": FN, "parallelism": f"replicas x{n_gpus}"}
 
 
 # --------------------------------------------------------------------------- GPU arm
@@ -282,20 +329,19 @@ def run_b200(args):
     torch.cuda.synchronize()
     t_prof = ev0.elapsed_time(ev1) / 1e3 / prof_steps
 
-    # ---- end to end through the public API: pinned host input, numpy output
-    pin_p = torch.from_numpy(p).pin_memory()
-    pin_c = torch.from_numpy(c).pin_memory()
+    # ---- end to end through the public API as a numpy caller uses it: numpy (pageable)
+    # input copied to the device and numpy output copied back inside the timed region
     # warm-up in the timed loop's own pattern: a caller that keeps the previous
     # result while the next call runs holds two pinned output blocks
     for _ in range(2):
-        u_np, cc_np = core_b200.irls_unwrap_2d(pin_p, pin_c, device=dev, **FN)
+        u_np, cc_np = core_b200.irls_unwrap_2d(p, c, device=dev, **FN)
     torch.cuda.synchronize()
     barrier(world)
     e2e_steps = max(1, min(args.steps, 3))
     t = time.perf_counter()
     ev0.record(stream)
     for _ in range(e2e_steps):
-        u_np, cc_np = core_b200.irls_unwrap_2d(pin_p, pin_c, device=dev, **FN)
+        u_np, cc_np = core_b200.irls_unwrap_2d(p, c, device=dev, **FN)
     ev1.record(stream)
     torch.cuda.synchronize()
     t_e2e = max(ev0.elapsed_time(ev1) / 1e3, time.perf_counter() - t)
@@ -383,13 +429,14 @@ def run_b200(args):
     out = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(t_dev / args.steps * 1e3, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": workload_name(args.shape) + " (one full unwrap per step, replica per GPU)",
-                      "grid": [H, W], "params": FN, "irls_iters": stats["irls_iters"],
-                      "pcg_iters": stats["cg_iters_total"],
-                      "l2": "inputs 134 MB and solver working set ~1.1 GB exceed the 126 MB L2",
-                      "parallelism": f"replicas x{world}"},
+           "config": dict(workload_config((H, W), args.shape, world),
+                          step="one full unwrap per step, one replica per GPU",
+                          irls_iters=stats["irls_iters"], pcg_iters=stats["cg_iters_total"],
+                          l2="inputs 134 MB and solver working set ~1.1 GB exceed the 126 MB L2"),
            "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(npx * 8),
-                   "d2h_bytes_per_step": int(npx * 6)},
+                   "d2h_bytes_per_step": int(npx * 6),
+                   "path": "core_b200.irls_unwrap_2d(numpy phase, numpy weight) -> numpy (u, conncomp); "
+                           "pageable host input, pinned staging for the output"},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches // 1,
            "stack": stack, "link": link, "accuracy": accuracy}
     if rank == 0:

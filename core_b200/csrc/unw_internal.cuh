@@ -71,6 +71,7 @@ struct InstState {
     float kmed;
     float shift;
     int n_labels;
+    int n_kneg, n_kpos;         // valid pixels whose cycle count is -inf / +inf (infinite phase)
     int pad_;
 };
 

@@ -4,10 +4,10 @@
 // from one file-scope device array instead of a caller-provided workspace.
 //
 // Why: some callers cannot allocate device memory at the point where they
-// need the operator -- code running inside another framework's CUDA-graph
-// capture or stream-ordered region, real-time loops that forbid allocation
-// after start-up, or plain C callers with no allocator of their own.  They
-// pass only inputs and outputs.
+// need the operator -- plain C or Fortran codes that have no device allocator
+// of their own, and real-time loops that must not allocate after start-up
+// (an allocation can fail under memory pressure in the middle of a run, and
+// releasing one with cudaFree synchronises the whole device).  They pass only inputs and outputs.
 //
 // Limits and rules:
 //  * the array holds UNW_NOALLOC_BYTES (16 MiB) per GPU that loads the
@@ -15,12 +15,17 @@
 //  * a grid must fit: H * W <= UNW_NOALLOC_MAX_PX float32 work values and
 //    each transform length within the usual limits; larger grids are
 //    rejected with UNW_E_UNSUPPORTED and a message;
+//  * r and z must be 16-byte aligned device pointers (the row kernels move
+//    four floats per access); others are rejected with UNW_E_ARG;
 //  * every call on a device uses the same array, so calls that overlap on
 //    the GPU (different streams, or threads without ordering) race; calls on
 //    one stream are ordered and safe;
 //  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress, with that device current) and caches it; make
-//    that first call before any stream capture;
+//    (cudaGetSymbolAddress, with that device current) and caches it for the
+//    life of the process; after cudaDeviceReset that cached address is stale,
+//    so a process that resets a device must not call this entry point again;
+//  * each call uploads the grid descriptor from host memory with
+//    cudaMemcpyAsync on the caller's stream;
 //  * nothing in this path calls cudaMalloc, cudaFree or any allocating
 //    library routine, and no host heap memory is used.
 #include <cuda_runtime.h>
@@ -113,6 +118,8 @@ bool pow2_ok(int n) { return n >= 256 && n <= 16384 && (n & (n - 1)) == 0; }
 extern "C" int unw_apply_preconditioner_noalloc(const float* r, int64_t H, int64_t W, float* z,
                                                 void* cuda_stream) {
     if (!r || !z) return unw_set_error(UNW_E_ARG, "null pointer");
+    if (((uintptr_t)r | (uintptr_t)z) & 15)
+        return unw_set_error(UNW_E_ARG, "r and z must be 16-byte aligned device pointers");
     if (H <= 0 || W <= 0) return unw_set_error(UNW_E_ARG, "bad shape");
     if (H * W > (int64_t)UNW_NOALLOC_MAX_PX)
         return unw_set_error(UNW_E_UNSUPPORTED,

@@ -26,8 +26,12 @@ __device__ __forceinline__ float cycles_f(float u, float ph) {
 }
 
 // ---------------------------------------------------------------- stats
+// Non-finite solution count (utils_unwrap2d.py:1659-1665) and the range of the
+// cycle counts k.  An infinite input phase on a valid pixel gives k = -inf or
+// +inf there (u is finite by now); those are counted apart and enter the median
+// as the smallest / largest values, as they do in np.median.
 __global__ void p_kstats(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
-    __shared__ double red[32];
+    __shared__ double red[32 * 3];
     __shared__ int smin, smax;
     const int g = find_grid(starts, n, blockIdx.x);
     const GridDev& G = grids[g];
@@ -40,13 +44,14 @@ __global__ void p_kstats(const GridDev* __restrict__ grids, const int* __restric
     if (threadIdx.x == 0) { smin = INT_MAX; smax = INT_MIN; }
     __syncthreads();
     int kmn = INT_MAX, kmx = INT_MIN;
-    double acc[1] = {0.0};
+    double acc[3] = {0.0, 0.0, 0.0};
     for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
         const int i = (int)(q / W), j = (int)(q - (long long)i * W);
         if (!G.valid[(size_t)i * P + j]) continue;
         const float u = U[(size_t)i * P + j];
         if (!isfinite(u)) { acc[0] += 1.0; continue; }
         float k = cycles_f(u, G.phase[(long long)i * G.phase_pitch + j]);
+        if (!isfinite(k)) { acc[k < 0.f ? 1 : 2] += 1.0; continue; }
         k = fminf(fmaxf(k, -1073741824.f), 1073741824.f);
         const int ki = (int)k;
         kmn = min(kmn, ki);
@@ -59,13 +64,24 @@ __global__ void p_kstats(const GridDev* __restrict__ grids, const int* __restric
     if ((threadIdx.x & 31) == 0) { atomicMin(&smin, kmn); atomicMax(&smax, kmx); }
     __syncthreads();
     if (threadIdx.x == 0) { atomicMin(&st->kmin, smin); atomicMax(&st->kmax, smax); }
-    if (arrive<1>(G, local, nct, acc, red)) {
-        finish_sum<1>(G, nct, acc, red);
+    if (arrive<3>(G, local, nct, acc, red)) {
+        finish_sum<3>(G, nct, acc, red);
         if (threadIdx.x == 0) {
             st->n_nonfinite = (int)acc[0];
-            const int kmin = __ldcg(&st->kmin), kmax = __ldcg(&st->kmax);
-            const long long range = (long long)kmax - (long long)kmin + 1;
-            st->hist_ok = (acc[0] == 0.0 && st->vcount > 0 && range >= 1 && range <= G.hist_cap) ? 1 : 0;
+            st->n_kneg = (int)acc[1];
+            st->n_kpos = (int)acc[2];
+            const double nfin = st->vcount - acc[1] - acc[2];
+            bool ok;
+            if (nfin > 0.0) {
+                const int kmin = __ldcg(&st->kmin), kmax = __ldcg(&st->kmax);
+                const long long range = (long long)kmax - (long long)kmin + 1;
+                ok = range >= 1 && range <= G.hist_cap;
+            } else {
+                st->kmin = 0;  // no finite count: empty histogram
+                st->kmax = -1;
+                ok = st->vcount > 0;
+            }
+            st->hist_ok = (acc[0] == 0.0 && ok) ? 1 : 0;
         }
     }
 }
@@ -82,6 +98,7 @@ __global__ void p_hist(const GridDev* __restrict__ grids, const int* __restrict_
     const long long npx = (long long)G.H * W;
     const float* __restrict__ U = ufinal(G, st);
     const int kmin = st->kmin, range = st->kmax - st->kmin + 1;
+    if (range <= 0) return;
     const bool small = range <= 2048;
     if (small) {
         for (int b = threadIdx.x; b < range; b += blockDim.x) sh[b] = 0;
@@ -90,7 +107,9 @@ __global__ void p_hist(const GridDev* __restrict__ grids, const int* __restrict_
     for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
         const int i = (int)(q / W), j = (int)(q - (long long)i * W);
         if (!G.valid[(size_t)i * P + j]) continue;
-        const int k = (int)cycles_f(U[(size_t)i * P + j], G.phase[(long long)i * G.phase_pitch + j]) - kmin;
+        const float kf = cycles_f(U[(size_t)i * P + j], G.phase[(long long)i * G.phase_pitch + j]);
+        if (!isfinite(kf)) continue;  // counted as -inf / +inf by p_kstats
+        const int k = (int)kf - kmin;
         if (k < 0 || k >= range) continue;
         if (small) atomicAdd(&sh[k], 1); else atomicAdd(&G.hist[k], 1);
     }
@@ -101,8 +120,10 @@ __global__ void p_hist(const GridDev* __restrict__ grids, const int* __restrict_
     }
 }
 
-// One CTA per grid: order statistics of the histogram -> np.median semantics
-// (mean of the two middle values), shift = float32(float32(2*kmed) * float32(pi)).
+// One CTA per grid: order statistics of the sorted cycle counts -> np.median
+// semantics (mean of the two middle values), shift = float32(float32(2*kmed) *
+// float32(pi)).  The sorted order is n_kneg times -inf, the histogram, then
+// n_kpos times +inf.
 __global__ void p_median(const GridDev* __restrict__ grids, int n) {
     __shared__ int s_lo, s_hi;
     __shared__ int wsum[32];
@@ -110,7 +131,10 @@ __global__ void p_median(const GridDev* __restrict__ grids, int n) {
     InstState* st = G.st;
     if (!post_ok(st)) return;
     const long long nv = (long long)st->vcount;
+    const long long nneg = st->n_kneg, nfin = nv - st->n_kneg - st->n_kpos;
     const long long plo = (nv - 1) / 2, phi = nv / 2;
+    const long long qlo = plo - nneg, qhi = phi - nneg;  // positions inside the histogram
+    const bool need_lo = qlo >= 0 && qlo < nfin, need_hi = qhi >= 0 && qhi < nfin;
     const int range = st->kmax - st->kmin + 1;
     if (threadIdx.x == 0) { s_lo = -1; s_hi = -1; }
     __syncthreads();
@@ -138,18 +162,20 @@ __global__ void p_median(const GridDev* __restrict__ grids, int n) {
         const long long incl = base + x + (wid > 0 ? wsum[wid - 1] : 0);
         const long long excl = incl - v;
         if (v > 0) {
-            if (plo >= excl && plo < incl) s_lo = b;
-            if (phi >= excl && phi < incl) s_hi = b;
+            if (qlo >= excl && qlo < incl) s_lo = b;
+            if (qhi >= excl && qhi < incl) s_hi = b;
         }
         base += wsum[nw - 1];
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        const float klo = (float)(s_lo + st->kmin), khi = (float)(s_hi + st->kmin);
+        const float inf = __int_as_float(0x7f800000);
+        const float klo = need_lo ? (float)(s_lo + st->kmin) : (qlo < 0 ? -inf : inf);
+        const float khi = need_hi ? (float)(s_hi + st->kmin) : (qhi < 0 ? -inf : inf);
         const float kmed = __fdiv_rn(__fadd_rn(klo, khi), 2.0f);
         st->kmed = kmed;
         st->shift = __fmul_rn(__fmul_rn(kmed, 2.0f), 3.14159274101257324f);
-        if (s_lo < 0 || s_hi < 0) st->hist_ok = 0;
+        if ((need_lo && s_lo < 0) || (need_hi && s_hi < 0)) st->hist_ok = 0;
     }
 }
 

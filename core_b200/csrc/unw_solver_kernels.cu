@@ -82,7 +82,7 @@ __global__ void k_state_init(const GridDev* __restrict__ grids, int n, UnwScalar
     s->cg_rel = sc.cg_rel;
     s->cg_total = 0;
     for (int i = 0; i < UNW_MAX_LOG; i++) s->cg_log[i] = 0;
-    s->n_nonfinite = 0; s->kmin = INT_MAX; s->kmax = INT_MIN; s->hist_ok = 1; s->kmed = 0.f; s->shift = 0.f;
+    s->n_nonfinite = 0; s->n_kneg = 0; s->n_kpos = 0; s->kmin = INT_MAX; s->kmax = INT_MIN; s->hist_ok = 1; s->kmed = 0.f; s->shift = 0.f;
     s->n_labels = 0;
     if (grids[g].H == 0) { s->irls_active = 0; s->hist_ok = 0; }
     *grids[g].counter = 0u;

@@ -14,8 +14,11 @@ conventions and error behaviour of insardev/insardev/utils_unwrap2d.py:1082:
   non-finite solution -> `RuntimeWarning` and (NaN, zeros).
 
 The solve runs entirely in libunwrap_b200.so (hand-written sm_100a kernels);
-PyTorch only provides device memory and the stream.  Devices other than CUDA
-are rejected: there is no CPU fallback.
+PyTorch only provides device memory and the stream.  A `device` that names the
+host or another accelerator (insardev's stack pipeline passes 'cpu' when its
+dask workers advertise no GPU) runs on the current CUDA device; the stats
+record the request.  There is no CPU fallback: without a CUDA device the call
+raises.
 """
 from __future__ import annotations
 
@@ -36,17 +39,34 @@ def _torch():
 
 
 def resolve_device(device, phase=None):
-    """'auto' / 'cuda' / 'cuda:N' / torch.device -> a CUDA torch.device (else raise)."""
+    """The CUDA torch.device a call runs on.
+
+    'auto' / None -> the device of a CUDA tensor input, else the current CUDA
+    device; 'cuda' / 'cuda:N' / torch.device('cuda', N) -> that device.  A host
+    or other accelerator request ('cpu', 'mps', 'tpu', ...) also runs on the
+    current CUDA device: insardev's stack pipeline passes the device it
+    resolved from its dask worker resources (Stack_unwrap2d.py:834-835, passed
+    on at :65), which is 'cpu' whenever the workers advertise no GPU, and this
+    implementation has only the CUDA path.  With no CUDA device visible the
+    call raises RuntimeError (there is no CPU fallback).
+    """
     torch = _torch()
     if isinstance(phase, torch.Tensor) and phase.is_cuda and device in ("auto", None):
         return phase.device
-    if device in ("auto", None):
+    dev = None
+    if device not in ("auto", None):
+        try:
+            dev = torch.device(device) if not isinstance(device, torch.device) else device
+        except (RuntimeError, TypeError):
+            dev = None  # e.g. 'tpu': not a torch device type here
+        if dev is not None and dev.type != "cuda":
+            dev = None
+    if dev is None:
         if not torch.cuda.is_available():
             raise RuntimeError("core_b200.irls_unwrap_2d needs a CUDA GPU; none is visible")
+        if isinstance(phase, torch.Tensor) and phase.is_cuda:
+            return phase.device
         return torch.device("cuda", torch.cuda.current_device())
-    dev = torch.device(device) if not isinstance(device, torch.device) else device
-    if dev.type != "cuda":
-        raise ValueError(f"core_b200.irls_unwrap_2d runs on CUDA devices only, got device={device!r}")
     if dev.index is None:
         dev = torch.device("cuda", torch.cuda.current_device())
     return dev
@@ -160,6 +180,8 @@ def irls_unwrap_2d(phase, weight=None, device='auto', max_iter=50, tol=1e-3,
                                ws.data_ptr(), ws.numel(), C.byref(st), stream)
         _lib.check(rc, "unw_solve_f32")
     stats = st.as_dict()
+    stats["device"] = str(dev)
+    stats["device_requested"] = str(device)
     if debug:
         _print_debug(H, W, stats)
     if st.status & _lib.UNW_S_ALL_NAN:
@@ -258,6 +280,8 @@ def irls_unwrap_2d_batch(phases, weights=None, device='auto', max_iter=50, tol=1
 
 def _print_debug(H, W, s):
     r0, r1, c0, c1 = s["bbox"]
+    if s.get("device_requested") not in (None, "auto", "None", s.get("device")):
+        print(f"  device {s['device_requested']!r} requested: solved on {s['device']}")
     print(f"  Cropped to bbox [{r0}:{r1}, {c0}:{c1}] = {r1 - r0}x{c1 - c0} (from {H}x{W})")
     for i, cg in enumerate(s["cg_iters"]):
         if i % 5 == 0:

@@ -282,15 +282,16 @@ UNW_API int unw_link_offsets(int32_t n, int32_t m, const int32_t* ei, const int3
 /*
  * Allocation-free variant of unw_apply_preconditioner.  It has no counterpart
  * in the reference.  It is for callers that cannot allocate device memory
- * where they need the operator (inside another framework's graph capture or
- * stream-ordered region, allocation-free real-time loops, C callers without
- * an allocator): its scratch is one 16 MiB device array that the library
- * holds on every GPU that loads it, so the caller passes only r and z (dense,
- * pitch W, device pointers).  Limit: H * W <= 3932160 and transform lengths
- * <= 16384, otherwise UNW_E_UNSUPPORTED.  All calls on a device share the
- * array: calls that overlap on the GPU race (order them on one stream).  The
- * first call on a device looks up the array's address; make it before any
- * stream capture.
+ * where they need the operator: C or Fortran codes with no device allocator
+ * of their own, and real-time loops that must not allocate after start-up.
+ * Its scratch is one 16 MiB device array that the library holds on every GPU
+ * that loads it, so the caller passes only r and z (dense, pitch W, device
+ * pointers, 16-byte aligned, else UNW_E_ARG).  Limit: H * W <= 3932160 and
+ * transform lengths <= 16384, otherwise UNW_E_UNSUPPORTED.  All calls on a
+ * device share the array: calls that overlap on the GPU race (order them on
+ * one stream).  The first call on a device looks up the array's address and
+ * caches it for the life of the process; it is not valid after
+ * cudaDeviceReset.
  */
 UNW_API int unw_apply_preconditioner_noalloc(const float* r, int64_t H, int64_t W, float* z,
                                              void* cuda_stream);

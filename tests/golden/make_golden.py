@@ -2,7 +2,7 @@
 
 Run in a container that holds the reference source tree (read-only):
 
-    python tests/golden/make_golden.py [--ref /root/reference] [--large]
+    python tests/golden/make_golden.py --ref <insardev checkout> (or INSARDEV_REF=<checkout>) [--large]
 
 It imports `insardev/insardev/utils_unwrap2d.py` through a synthetic `insardev`
 package with two shims: a stub `insardev.BatchCore` (the function imports it
@@ -140,6 +140,21 @@ def cases_small():
         out.append((f"tiny_{h}x{w}", ph, wt, dict(FN_DEFAULTS, conncomp_size=1)))
     ph = np.full((8, 8), np.nan, np.float32)
     out.append(("all_nan", ph, None, FN_DEFAULTS))
+    # non-finite phase on valid pixels: wrap(inf) = NaN gradients reach the DCT
+    # initial solve (zero-filled, utils_unwrap2d.py:1498-1502), the IRLS weights
+    # and the PCG start (non-finite residual, :1418-1419), and the circular means
+    # of the component that holds the pixel
+    p, c, _ = gen_g1(64, 72, seed=10)
+    p[10, 10] = np.inf
+    p[40, 50] = -np.inf
+    out.append(("nonfinite_phase", p, c, FN_DEFAULTS))
+    # the same with the infinite pixel cut off from the rest (its own 1-pixel component)
+    p, c, _ = gen_g1(48, 40, seed=11, nan_fraction=0.0)
+    p[19:22, 19:22] = np.nan
+    p[20, 20] = np.inf
+    c = c.copy()
+    c[np.isnan(p)] = np.nan
+    out.append(("nonfinite_isolated", p, c, dict(FN_DEFAULTS, conncomp_size=5)))
     return out
 
 
@@ -169,7 +184,8 @@ def save_large(name, gen, gen_args, params, phase, u, cc, iters, secs, precision
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("INSARDEV_REF"), required="INSARDEV_REF" not in os.environ,
+                    help="root of the insardev source checkout (default: $INSARDEV_REF)")
     ap.add_argument("--large", action="store_true", help="also the 1024^2 grids")
     ap.add_argument("--xlarge", action="store_true", help="also the 4096^2 fault grid (~8 min)")
     ap.add_argument("--xlarge64", action="store_true",

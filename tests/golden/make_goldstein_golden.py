@@ -2,7 +2,7 @@
 
 Run in a container that holds the reference source tree (read-only):
 
-    python tests/golden/make_goldstein_golden.py [--ref /root/reference]
+    python tests/golden/make_goldstein_golden.py --ref <insardev checkout> (or INSARDEV_REF=<checkout>)
 
 It loads `insardev/insardev/utils_goldstein.py` as a plain module (its
 functions import numpy and torch only) and runs `goldstein_pytorch` on the CPU
@@ -60,7 +60,8 @@ def make_case(H, W, seed, nan_fraction):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("INSARDEV_REF"), required="INSARDEV_REF" not in os.environ,
+                    help="root of the insardev source checkout (default: $INSARDEV_REF)")
     a = ap.parse_args()
     import torch
     ref = load_reference(a.ref)

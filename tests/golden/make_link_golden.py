@@ -2,7 +2,7 @@
 
 Run in a container that holds the reference source tree (read-only):
 
-    python tests/golden/make_link_golden.py [--ref /root/reference]
+    python tests/golden/make_link_golden.py --ref <insardev checkout> (or INSARDEV_REF=<checkout>)
 
 The reference functions `find_component_connections_fast` and
 `connect_components_ilp_fast` (insardev/insardev/utils_unwrap2d.py:195-444,
@@ -473,7 +473,8 @@ CASES = [
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("INSARDEV_REF"), required="INSARDEV_REF" not in os.environ,
+                    help="root of the insardev source checkout (default: $INSARDEV_REF)")
     a = ap.parse_args()
     install_shapely()
     install_ortools()

@@ -70,10 +70,29 @@ def test_python_boundary_validation_without_gpu():
     import core_b200
     with pytest.raises(ValueError):
         core_b200.irls_unwrap_2d(np.zeros((2, 3, 4), np.float32))
-    with pytest.raises(ValueError):
+
+
+def test_host_device_requests_run_on_the_cuda_device(monkeypatch):
+    """insardev's stack pipeline passes the device it resolved from its dask workers
+    (Stack_unwrap2d.py:834-835, then :65), 'cpu' when they advertise no GPU: the
+    drop-in runs such calls on the current CUDA device instead of failing, and
+    raises RuntimeError when no CUDA device is visible (no CPU fallback)."""
+    import torch
+
+    from core_b200.irls import resolve_device
+    monkeypatch.setattr(torch.cuda, "is_available", lambda: True)
+    monkeypatch.setattr(torch.cuda, "current_device", lambda: 3)
+    for req in ("cpu", "mps", "tpu", "auto", None, torch.device("cpu")):
+        assert resolve_device(req) == torch.device("cuda", 3), req
+    assert resolve_device("cuda:1") == torch.device("cuda", 1)
+    assert resolve_device("cuda") == torch.device("cuda", 3)
+    monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
+    for req in ("cpu", "auto"):
+        with pytest.raises(RuntimeError):
+            resolve_device(req)
+    import core_b200
+    with pytest.raises(RuntimeError):
         core_b200.irls_unwrap_2d(np.zeros((4, 4), np.float32), device="cpu")
-    with pytest.raises(ValueError):
-        core_b200.irls_unwrap_2d(np.zeros((4, 4), np.float32), device="mps")
 
 
 def test_adjoint_rejects_bad_args_without_gpu():

@@ -29,6 +29,9 @@ def test_oracle_matches_reference(name):
         return
     assert st.irls_iters == int(d["iters"])
     assert (cycle_map(u, p) == cycle_map(ur, p))[v].all()
+    v &= np.isfinite(ur)  # an infinite input phase leaves its component NaN
+    if not v.any():
+        return
     e = (u - ur)[v].astype(np.float64)
     rms = np.sqrt(np.mean((e - e.mean()) ** 2))
     assert rms <= (1e-6 if dt == np.float64 else 1e-4)
