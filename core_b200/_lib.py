@@ -24,6 +24,9 @@ UNW_F_CONGRUENT = 1
 UNW_F_NO_GRAPH = 2
 UNW_F_PROFILE = 4
 UNW_F_FIXED_ITERS = 8
+UNW_F_MIXED = 16
+UNW_F_COL_TC = 32
+UNW_F_COL_FFT = 64
 
 PROF_NAMES = ["bbox", "setup", "row_rho", "col", "row_inv", "matvec", "row_upd", "row_r0", "head", "elem", "post"]
 PROF_N = len(PROF_NAMES)
@@ -32,6 +35,7 @@ UNW_S_DCT_INIT_NONFINITE = 1
 UNW_S_REVERTED = 2
 UNW_S_NONFINITE_OUT = 4
 UNW_S_ALL_NAN = 8
+UNW_S_TC_TIMEOUT = 16
 
 
 class UnwParams(C.Structure):
@@ -45,7 +49,9 @@ class UnwStats(C.Structure):
                 ("n_components", C.c_int32), ("n_labels", C.c_int32), ("status", C.c_int32),
                 ("bbox", C.c_int32 * 4), ("rel_change", C.c_double), ("best_residual", C.c_double),
                 ("k_median", C.c_double), ("cg_iters", C.c_int32 * 64),
-                ("prof_ms", C.c_float * 16), ("prof_launches", C.c_int32 * 16)]
+                ("prof_ms", C.c_float * 16), ("prof_launches", C.c_int32 * 16),
+                ("col_path", C.c_int32), ("tune_ms", C.c_float * 2), ("pad_", C.c_int32),
+                ("resid_rel", C.c_double)]
 
     def as_dict(self):
         n = min(self.irls_iters, 64)
@@ -54,7 +60,8 @@ class UnwStats(C.Structure):
                     n_labels=self.n_labels, status=self.status, bbox=tuple(self.bbox),
                     rel_change=self.rel_change, best_residual=self.best_residual,
                     k_median=self.k_median, cg_iters=list(self.cg_iters[:n]),
-                    prof_ms=list(self.prof_ms[:PROF_N]), prof_launches=list(self.prof_launches[:PROF_N]))
+                    prof_ms=list(self.prof_ms[:PROF_N]), prof_launches=list(self.prof_launches[:PROF_N]),
+                    col_path=self.col_path, tune_ms=list(self.tune_ms), resid_rel=self.resid_rel)
 
 
 UNW_LINK_C_LINE = 1
@@ -95,6 +102,8 @@ SIGNATURES = {
                                       C.c_void_p, C.c_size_t, C.c_void_p]),
     "unw_apply_preconditioner": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
                                            C.c_size_t, C.c_void_p]),
+    "unw_apply_preconditioner_mixed": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int32,
+                                                 C.c_void_p, C.c_size_t, C.c_void_p]),
     "unw_apply_preconditioner_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "unw_adjoint_workspace_bytes": (C.c_size_t, [C.c_int64, C.c_int64]),
     "unw_goldstein_workspace_bytes": (C.c_size_t, [C.c_int64, C.c_int64, C.c_int32, C.c_int32]),

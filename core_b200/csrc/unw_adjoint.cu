@@ -23,7 +23,7 @@
     for (int i = (local); i < (G).H; i += (nct))         \
         for (int j = threadIdx.x; j < (G).W; j += blockDim.x)
 
-// u (forward output, NaN outside the valid pixels) -> U0 on the crop, NaN -> 0;
+// u (forward output, NaN outside the valid pixels) -> iterate pair (U0, L0 = 0) on the crop, NaN -> 0;
 // dL/dout -> z (unused by the solver), 0 at invalid pixels.
 __global__ void k_adj_load(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n,
                            const float* __restrict__ u, long long up, const float* __restrict__ gu, long long gp) {
@@ -38,6 +38,7 @@ __global__ void k_adj_load(const GridDev* __restrict__ grids, const int* __restr
         const float gv = gu[gi * gp + gj];
         const bool v = G.valid[o] != 0;
         G.U0[o] = (v && isfinite(uv)) ? uv : 0.f;
+        G.L0[o] = 0.f;
         G.z[o] = (v && isfinite(gv)) ? gv : 0.f;
     }
 }
@@ -62,7 +63,8 @@ __device__ __forceinline__ double dcircmean(double s, double c, float x) {
     return d > 0.0 ? (c * (double)cosf(x) + s * (double)sinf(x)) / d : 0.0;
 }
 
-// right-hand side of the adjoint solve, b = G' (valid) / 0, and x0 = 0 in U0
+// right-hand side of the adjoint solve, b = G' (valid) / 0, and x0 = 0 in (U0, L0); the
+// PCG then accumulates lambda = x - x0 in D
 __global__ void k_adj_rhs(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
     const int g = find_grid(starts, n, blockIdx.x);
     const GridDev& G = grids[g];
@@ -82,6 +84,7 @@ __global__ void k_adj_rhs(const GridDev* __restrict__ grids, const int* __restri
         }
         G.b[o] = v;
         G.U0[o] = 0.f;
+        G.L0[o] = 0.f;
     }
 }
 
@@ -106,7 +109,7 @@ __global__ void k_adj_grad(const GridDev* __restrict__ grids, const int* __restr
     const size_t cap = (size_t)G.lab_cap;
     const int nlab = G.st->n_labels;
     const int H = G.H, W = G.W, P = G.P;
-    const float* __restrict__ lam = G.U0;
+    const float* __restrict__ lam = G.D;   // the adjoint PCG's x - x0 with x0 = 0
     const float* __restrict__ us = G.U1;
     UNW_ROWS_LOOP(G, local, nct) {
         const size_t o = (size_t)i * P + j;

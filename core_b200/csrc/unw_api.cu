@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <array>
 #include <map>
+#include <mutex>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -142,8 +143,9 @@ HostPlan make_plan(int N) {
 // ------------------------------------------------------------ layout
 struct GridLayout {
     size_t st, counter, part, tw_r, dw_r, ch_r, hs_r, cos_r, tw_c, dw_c, ch_c, hs_c, cos_c;
-    size_t arr[16];          // gx gy wx wy | wIx wIy b r z p0 p1 Ap T | U0 U1 Ub
+    size_t arr[20];          // gx gy wx wy | wIx wIy b r z p0 p1 Ap T | U0 U1 Ub | L0 L1 Lb D
     size_t valid, hist, tilecnt;
+    size_t tc;               // split DCT matrices of the tensor-core column pass (H0 <= UNW_TC_MAX_H), else 0
     size_t post_parent, post_lab, post_csum, post_ccount, post_remap, post_adj;
     size_t end;
     long long P0, max_ctas, lab_cap, ntiles_max;
@@ -186,8 +188,9 @@ GridLayout grid_layout(long long H0, long long W0) {
     L.dw_c = take(sizeof(float2) * H0);
     L.ch_c = take(sizeof(float2) * H0);
     L.cos_c = take(sizeof(float) * H0);
-    for (int a = 0; a < 16; a++) L.arr[a] = take(A);
+    for (int a = 0; a < 20; a++) L.arr[a] = take(A);
     L.valid = take((size_t)H0 * L.P0);
+    L.tc = H0 <= UNW_TC_MAX_H ? take(unw_tc_table_bytes((int)H0)) : 0;
     L.hist = take(sizeof(int) * HIST_CAP);
     L.ntiles_max = (H0 * W0 + 4095) / 4096;
     L.tilecnt = take(sizeof(int) * (size_t)L.ntiles_max);
@@ -234,6 +237,7 @@ struct Shape {
     size_t row_smem = 0, col_smem = 0;
     int row_p2 = 0, col_p2 = 0;   // power-of-two register-FFT paths (length), 0 = generic
     int row_bl = 0, col_bl = 0;   // Bluestein register-FFT paths (FFT length M), 0 = not used
+    int col_tc = 0;               // tensor-core column pass (mixed precision), chosen by the autotuner
 };
 
 int elem_ctas(long long npx) {
@@ -285,6 +289,11 @@ struct Prof {
     }
 };
 
+struct TuneResult {
+    int tc = 0;
+    float ms_fft = 0.f, ms_tc = 0.f;   // per launch of each column pass
+};
+
 struct Solver {
     int n = 0;
     Prof prof;
@@ -295,6 +304,8 @@ struct Solver {
     GridDev* dg = nullptr;
     int* dstarts = nullptr;
     Shape sh;
+    TcMaps maps;                 // tensor maps of the split DCT matrices (col_tc)
+    TuneResult tune;             // autotuner timings of the column pass (mixed precision)
     UnwScalars sc{};
     const int* ds(int kind) const { return dstarts + (size_t)kind * (n + 1); }
 };
@@ -330,6 +341,7 @@ cudaError_t L_rowi(Solver& S, int mode) {
                               S.ds(KS_ROWPAIR), S.n);
 }
 cudaError_t L_col(Solver& S, int mode) {
+    if (S.sh.col_tc) return unw_launch_col_tc(mode, S.total[KS_TC], S.s, S.dg, S.ds(KS_TC), S.n, &S.maps);
     if (S.sh.col_p2) return unw_launch_col_p2(S.sh.col_p2, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n);
     if (S.sh.col_bl) return unw_launch_col_bl(S.sh.col_bl, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n);
     return unw_launch_col(mode, S.sh.col_T, S.sh.col_emax, S.total[KS_COL], S.sh.col_smem, S.s, S.dg, S.ds(KS_COL),
@@ -446,6 +458,48 @@ std::array<int, 4> group_key(int H, int W) {
     return k;
 }
 
+// Autotuner of the mixed-precision form: times the FFT column pass against the
+// tensor-core one on the group's own buffers (DCT initial-solve mode, which has no
+// PCG gate; two warm-up and three timed launches of each on the solve stream) and
+// returns 1 when the tensor cores are faster.  The choice is cached per device and
+// (H, max W) for the life of the process; it runs before any graph capture.
+TuneResult autotune_col(Solver& S, int H, int W) {
+    static std::mutex mu;
+    static std::map<std::array<int, 3>, TuneResult> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const std::array<int, 3> key{dev, H, W};
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    cudaEvent_t e[4];
+    for (auto& x : e) cudaEventCreate(&x);
+    bool ok = true;
+    for (int tc = 0; tc < 2; tc++) {
+        S.sh.col_tc = tc;
+        for (int r = 0; r < 2; r++) ok &= L_col(S, 0) == cudaSuccess;
+        cudaEventRecord(e[2 * tc], S.s);
+        for (int r = 0; r < 3; r++) ok &= L_col(S, 0) == cudaSuccess;
+        cudaEventRecord(e[2 * tc + 1], S.s);
+    }
+    S.sh.col_tc = 0;
+    TuneResult res;
+    float t_fft = 0.f, t_tc = 0.f;
+    if (ok && cudaEventSynchronize(e[3]) == cudaSuccess && cudaEventElapsedTime(&t_fft, e[0], e[1]) == cudaSuccess &&
+        cudaEventElapsedTime(&t_tc, e[2], e[3]) == cudaSuccess) {
+        res.ms_fft = t_fft / 3.f;
+        res.ms_tc = t_tc / 3.f;
+        res.tc = t_tc < t_fft ? 1 : 0;
+    }
+    cudaGetLastError();
+    for (auto& x : e) cudaEventDestroy(x);
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = res;
+    return res;
+}
+
 // Per-grid descriptors, FFT plans, launch shapes, CTA prefix arrays and
 // tables for grids cropped to bbox (r0, r1, c0, c1 per grid).
 int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const std::vector<int>& bbox,
@@ -490,9 +544,10 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
         G.st = (InstState*)(gb + L.st);
         G.counter = (unsigned*)(gb + L.counter);
         G.part = (double*)(gb + L.part);
-        float** arrs[16] = {&G.gx, &G.gy, &G.wx, &G.wy, &G.wIx, &G.wIy, &G.b, &G.r,
-                            &G.z, &G.p0, &G.p1, &G.Ap, &G.T, &G.U0, &G.U1, &G.Ub};
-        for (int a = 0; a < 16; a++) *arrs[a] = (float*)(gb + L.arr[a]);
+        float** arrs[20] = {&G.gx, &G.gy, &G.wx, &G.wy, &G.wIx, &G.wIy, &G.b, &G.r,
+                            &G.z, &G.p0, &G.p1, &G.Ap, &G.T, &G.U0, &G.U1, &G.Ub,
+                            &G.L0, &G.L1, &G.Lb, &G.D};
+        for (int a = 0; a < 20; a++) *arrs[a] = (float*)(gb + L.arr[a]);
         G.valid = (uint8_t*)(gb + L.valid);
         G.sH = (const float*)(gb + L.cos_c);
         G.sW = (const float*)(gb + L.cos_r);
@@ -579,12 +634,29 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
             S.sh.col_bl = mh;
             for (int g = 0; g < n; g++) S.hg[g].col_nseq = unw_bl_col_nseq(mh);
         }
-        // persistent column pass: as many CTAs as fit on the SMs (<= 2048 threads, 4 CTAs)
+        // persistent column pass: 148 x min(4, 2048 / threads) CTAs.  This is more than the
+        // register limit lets reside at once (2 per SM at 512 threads), so a second wave starts
+        // as first-wave CTAs finish; measured at 4096^2 that beats sizing the grid to the
+        // resident count (102 us vs 113 us per launch), as the late CTAs fill the tail
         const int cthreads = S.sh.col_p2 ? S.sh.col_p2 / 16 * unw_p2_col_nseq(S.sh.col_p2)
                              : S.sh.col_bl ? S.sh.col_bl / 16 * unw_bl_col_nseq(S.sh.col_bl)
                                            : S.sh.col_T;
         const int per_sm = std::max(1, std::min(4, 2048 / std::max(cthreads, 1)));
         for (int g = 0; g < n; g++) S.hg[g].col_ctas = NUM_SMS * per_sm;
+    }
+    // tensor-core column pass (mixed precision): every grid of the group has the same
+    // H <= UNW_TC_MAX_H (one pair of DCT matrices for the launch)
+    int tc_h = 0;
+    if (prm->flags & UNW_F_MIXED) {
+        for (int g = 0; g < n; g++) {
+            const int h = S.hg[g].H;
+            if (h == 0) continue;
+            if (tc_h == 0) tc_h = h;
+            else if (tc_h != h) { tc_h = -1; break; }
+        }
+        if (tc_h < 16 || tc_h > UNW_TC_MAX_H || (prm->flags & UNW_F_COL_FFT)) tc_h = 0;
+        for (int g = 0; g < n && tc_h > 0; g++)
+            if (S.hg[g].H > 0 && (S.hg[g].P & 3)) tc_h = 0;  // the pass moves float4 groups of rows
     }
     // CTA prefix arrays
     S.starts.assign((size_t)(KS_NKIND + 1) * (n + 1), 0);
@@ -593,7 +665,8 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
         int acc = 0;
         for (int g = 0; g < n; g++) {
             S.starts[(size_t)k * (n + 1) + g] = acc;
-            acc += kind_ctas(S.hg[g], k);
+            if (k == KS_TC) acc += (tc_h > 0 && S.hg[g].H > 0) ? unw_tc_ctas(S.hg[g].H, S.hg[g].W) : 0;
+            else acc += kind_ctas(S.hg[g], k);
         }
         S.starts[(size_t)k * (n + 1) + n] = acc;
         S.total[k] = acc;
@@ -613,7 +686,28 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
         if (G.pcol.blue) CK(unw_launch_hspec(pick_threads(pcol[g].n, pcol[g].cap), pcol[g].emax, G.pcol, s));
         CK(cudaMemsetAsync(G.hist, 0, sizeof(int) * HIST_CAP, s));
     }
-
+    if (tc_h > 0) {
+        char* tab = base + B.base[idx[0]] + B.g[idx[0]].tc;
+        const cudaError_t te = B.g[idx[0]].tc ? unw_tc_prepare(tc_h, tab, &S.maps, s) : cudaErrorInvalidValue;
+        if (te == cudaSuccess) {
+            if (prm->flags & UNW_F_COL_TC) {
+                S.sh.col_tc = 1;
+            } else {
+                int W0 = 0;
+                for (int g = 0; g < n; g++) W0 = std::max(W0, S.hg[g].W);
+                S.tune = autotune_col(S, tc_h, W0);
+                S.sh.col_tc = S.tune.tc;
+            }
+        }
+        cudaGetLastError();
+    }
+    bool any_grid = false;
+    for (int g = 0; g < n; g++) any_grid |= S.hg[g].H > 0;
+    if ((prm->flags & UNW_F_MIXED) && (prm->flags & UNW_F_COL_TC) && !S.sh.col_tc && any_grid) {
+        return set_err(UNW_E_UNSUPPORTED, "tensor-core column pass requested but unavailable for this grid "
+                                          "(all grids need the same H <= %d rows and a pitch of whole float4 groups)",
+                       UNW_TC_MAX_H);
+    }
     return UNW_OK;
 }
 
@@ -663,6 +757,11 @@ int solve_group(const std::vector<int>& idx, const unw_grid* grids, const std::v
                 if (!any) break;
             }
         }
+
+        // float64 residual of the final system (mixed-precision form), before the
+        // post-processing scratch overlays the weights
+        if (prm->flags & UNW_F_MIXED)
+            PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_RESID, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
 
         // 6. post-processing (utils_unwrap2d.py:1659-1757)
         PL(UNW_PROF_POST, unw_launch_post(UNW_P_KSTATS, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
@@ -732,6 +831,10 @@ int solve_group(const std::vector<int>& idx, const unw_grid* grids, const std::v
             o.best_residual = st.best_residual;
             o.k_median = st.kmed;
             for (int i = 0; i < 64 && i < UNW_MAX_LOG; i++) o.cg_iters[i] = G.H ? st.cg_log[i] : 0;
+            o.col_path = S.sh.col_tc;
+            o.tune_ms[0] = S.tune.ms_fft;
+            o.tune_ms[1] = S.tune.ms_tc;
+            o.resid_rel = st.resid_rel;
         }
     }
     if (stats && S.prof.on) S.prof.collect(stats[0].prof_ms, stats[0].prof_launches);
@@ -897,7 +1000,8 @@ int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_
     CK(unw_launch_post(UNW_P_TILESCAN, n, s, S.dg, nullptr, n, S.sc, S.hg.data()));
     CK(unw_launch_post(UNW_P_LABEL, nt, s, S.dg, S.ds(KS_NKIND), n, S.sc, S.hg.data()));
     CK(unw_launch_post(UNW_P_ACCUM, ne, s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
-    // 3. adjoint right-hand side through the alignment, then lambda = A^+ G' (x0 = 0, U0)
+    // 3. adjoint right-hand side through the alignment, then lambda = A^+ G' (x0 = 0 in U0/L0,
+    //    lambda accumulated in D)
     CK(cudaMemsetAsync(S.hg[0].adj, 0, sizeof(double) * (size_t)S.hg[0].lab_cap, s));
     CK(unw_launch_adj(UNW_A_LSUM, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
     CK(unw_launch_adj(UNW_A_RHS, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
@@ -1070,6 +1174,39 @@ int unw_apply_preconditioner(const float* r, int64_t H, int64_t W, float* z, voi
     CK(L_col(S, 0));
     CK(L_rowi(S, 3));
     return UNW_OK;
+}
+
+int unw_apply_preconditioner_mixed(const float* r, int64_t H, int64_t W, float* z, int32_t col_path,
+                                   void* workspace, size_t workspace_bytes, void* cuda_stream) {
+    if (!r || !z) return set_err(UNW_E_ARG, "null pointer");
+    if (col_path < -1 || col_path > 1) return set_err(UNW_E_ARG, "col_path must be -1, 0 or 1");
+    if (H <= 0 || W <= 0) return set_err(UNW_E_ARG, "bad shape %lld x %lld", (long long)H, (long long)W);
+    if (!workspace) return set_err(UNW_E_ARG, "workspace is NULL");
+    long long h = H, w = W;
+    BatchLayout B = batch_layout(1, &h, &w);
+    char* base = (char*)up((size_t)workspace, ALIGN);
+    if ((size_t)(base - (char*)workspace) + B.total - ALIGN > workspace_bytes)
+        return set_err(UNW_E_WORKSPACE, "workspace %zu bytes < %zu needed", workspace_bytes, B.total);
+    unw_grid q{};
+    q.phase_pitch = W;
+    q.weight_pitch = W;
+    q.H = H;
+    q.W = W;
+    unw_params prm{};
+    prm.epsilon = 1e-2f;
+    prm.flags = UNW_F_MIXED | (col_path == 1 ? UNW_F_COL_TC : 0) | (col_path == 0 ? UNW_F_COL_FFT : 0);
+    std::vector<int> bbox = {0, (int)H, 0, (int)W};
+    Solver S;
+    int rc = prepare(S, std::vector<int>{0}, &q, bbox, &prm, base, B, (cudaStream_t)cuda_stream, true, 0, 0);
+    if (rc) return rc;
+    GridDev& G = S.hg[0];
+    G.r = const_cast<float*>(r); G.z = z;
+    rc = op_upload(S);
+    if (rc) return rc;
+    CK(L_rowf(S, 3, 0, 0));
+    CK(L_col(S, 0));
+    CK(L_rowi(S, 3));
+    return S.sh.col_tc ? 1 : 0;
 }
 
 }  // extern "C"

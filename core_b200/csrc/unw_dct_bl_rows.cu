@@ -24,7 +24,8 @@ __device__ __forceinline__ float f4at(const float4& v, int c) {
 }
 
 // x += alpha p, r -= alpha Ap at columns j..j+3 of row i (the reference's PCG
-// update, utils_unwrap2d.py:1445-1459, same operations as rowfwd_value mode 2).
+// update, utils_unwrap2d.py:1445-1459, same operations as rowfwd_value mode 2;
+// x is the PCG correction D).
 // Rows are 128-byte aligned with a pitch of whole float4 groups, so a group
 // starting below W stays inside the row; columns >= W are updated but do not
 // enter the norms.
@@ -65,7 +66,8 @@ __global__ void __launch_bounds__(BL::T, bl_min_blocks<BL::T>()) k_rowf_bl(const
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
     const int t = threadIdx.x;
-    float* U = (it & 1) ? G.U0 : G.U1;
+    float* U = rowfwd_x<MODE>(G, it);  // x0 of this IRLS iteration, or D in mode 2
+    const float* Lo = rowfwd_lo(G, it);
     const float* pk = (MODE == 2) ? G.p0 : nullptr;
     const float alpha = (MODE == 2) ? st->alpha : 0.f;
     const float2* __restrict__ dw = G.prow.dctw;
@@ -84,8 +86,8 @@ __global__ void __launch_bounds__(BL::T, bl_min_blocks<BL::T>()) k_rowf_bl(const
             }
         } else {
             for (int j = t; j < W; j += T) {
-                const float a = rowfwd_value<MODE>(G, U, pk, alpha, i0, j, acc);
-                const float b = has1 ? rowfwd_value<MODE>(G, U, pk, alpha, i1, j, acc) : 0.f;
+                const float a = rowfwd_value<MODE>(G, U, Lo, pk, alpha, i0, j, acc);
+                const float b = has1 ? rowfwd_value<MODE>(G, U, Lo, pk, alpha, i1, j, acc) : 0.f;
                 sm[BL::pos(mk_perm(j, W))] = make_float2(a, b);
             }
         }

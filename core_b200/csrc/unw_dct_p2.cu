@@ -31,8 +31,9 @@ __device__ __forceinline__ float f4get(const float4& v, int c) {
 
 // Four consecutive source values of row i (columns j..j+3) of the row-forward pass.
 template <int MODE>
-__device__ __forceinline__ float4 rowf_vals4(const GridDev& G, float* __restrict__ U, const float* __restrict__ pk,
-                                             float alpha, int i, int j, double (&acc)[2]) {
+__device__ __forceinline__ float4 rowf_vals4(const GridDev& G, float* __restrict__ U, const float* __restrict__ Lo,
+                                             const float* __restrict__ pk, float alpha, int i, int j,
+                                             double (&acc)[2]) {
     const size_t o = (size_t)i * G.P + j;
     if (MODE == 2) {
         const float4 x = ld4f(U, o), p = ld4f(pk, o), r = ld4f(G.r, o), ap = ld4f(G.Ap, o);
@@ -49,26 +50,29 @@ __device__ __forceinline__ float4 rowf_vals4(const GridDev& G, float* __restrict
     } else if (MODE == 3) {
         return ld4f(G.r, o);
     } else if (MODE == 1) {
-        // r = b - A x at columns j..j+3 (x = U), A in the reference's op order
+        // r = b - A x0 at columns j..j+3, neighbour differences from the pair (rowfwd_value mode 1)
         const int H = G.H, W = G.W, P = G.P;
-        const float4 x4 = ld4f(U, o), b4 = ld4f(G.b, o), wx4 = ld4f(G.wIx, o), wy4 = ld4f(G.wIy, o);
-        const float4 xu4 = i > 0 ? ld4f(U, o - P) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 wyu4 = i > 0 ? ld4f(G.wIy, o - P) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 xd4 = i < H - 1 ? ld4f(U, o + P) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float xl = j > 0 ? U[o - 1] : 0.f, wxl = j > 0 ? G.wIx[o - 1] : 0.f;
-        const float xr = j + 4 < W ? U[o + 4] : 0.f;
+        const float4 x4 = ld4f(U, o), l4 = ld4f(Lo, o), b4 = ld4f(G.b, o), wx4 = ld4f(G.wIx, o), wy4 = ld4f(G.wIy, o);
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 xu4 = i > 0 ? ld4f(U, o - P) : z4, lu4 = i > 0 ? ld4f(Lo, o - P) : z4;
+        const float4 wyu4 = i > 0 ? ld4f(G.wIy, o - P) : z4;
+        const float4 xd4 = i < H - 1 ? ld4f(U, o + P) : z4, ld4 = i < H - 1 ? ld4f(Lo, o + P) : z4;
+        const float xl = j > 0 ? U[o - 1] : 0.f, ll = j > 0 ? Lo[o - 1] : 0.f;
+        const float wxl = j > 0 ? G.wIx[o - 1] : 0.f;
+        const float xr = j + 4 < W ? U[o + 4] : 0.f, lr = j + 4 < W ? Lo[o + 4] : 0.f;
         const float xs[6] = {xl, x4.x, x4.y, x4.z, x4.w, xr};
+        const float ls[6] = {ll, l4.x, l4.y, l4.z, l4.w, lr};
         const float wxs[5] = {wxl, wx4.x, wx4.y, wx4.z, wx4.w};
         float out[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int jj = j + q;
-            const float xc = xs[q + 1];
+            const float xc = xs[q + 1], lc = ls[q + 1];
             float res = 0.f;
-            if (jj > 0) res = fsub(res, fmul(fsub(xc, xs[q]), wxs[q]));
-            if (jj < W - 1) res = fadd(res, fmul(fsub(xs[q + 2], xc), wxs[q + 1]));
-            if (i > 0) res = fsub(res, fmul(fsub(xc, f4get(xu4, q)), f4get(wyu4, q)));
-            if (i < H - 1) res = fadd(res, fmul(fsub(f4get(xd4, q), xc), f4get(wy4, q)));
+            if (jj > 0) res = fsub(res, fmul(pair_diff(xc, lc, xs[q], ls[q]), wxs[q]));
+            if (jj < W - 1) res = fadd(res, fmul(pair_diff(xs[q + 2], ls[q + 2], xc, lc), wxs[q + 1]));
+            if (i > 0) res = fsub(res, fmul(pair_diff(xc, lc, f4get(xu4, q), f4get(lu4, q)), f4get(wyu4, q)));
+            if (i < H - 1) res = fadd(res, fmul(pair_diff(f4get(xd4, q), f4get(ld4, q), xc, lc), f4get(wy4, q)));
             const float val = fsub(f4get(b4, q), -res);
             out[q] = val;
             acc[0] += isfinite(val) ? 0.0 : 1.0;
@@ -76,13 +80,14 @@ __device__ __forceinline__ float4 rowf_vals4(const GridDev& G, float* __restrict
         }
         const float4 r4 = make_float4(out[0], out[1], out[2], out[3]);
         st4f(G.r, o, r4);
+        st4f(G.D, o, z4);
         return r4;
     } else {
         float4 v;
-        v.x = rowfwd_value<MODE>(G, U, pk, alpha, i, j, acc);
-        v.y = rowfwd_value<MODE>(G, U, pk, alpha, i, j + 1, acc);
-        v.z = rowfwd_value<MODE>(G, U, pk, alpha, i, j + 2, acc);
-        v.w = rowfwd_value<MODE>(G, U, pk, alpha, i, j + 3, acc);
+        v.x = rowfwd_value<MODE>(G, U, Lo, pk, alpha, i, j, acc);
+        v.y = rowfwd_value<MODE>(G, U, Lo, pk, alpha, i, j + 1, acc);
+        v.z = rowfwd_value<MODE>(G, U, Lo, pk, alpha, i, j + 2, acc);
+        v.w = rowfwd_value<MODE>(G, U, Lo, pk, alpha, i, j + 3, acc);
         return v;
     }
 }
@@ -102,7 +107,8 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowf_p2(const 
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, P = G.P;
     const int t = threadIdx.x;
-    float* U = (it & 1) ? G.U0 : G.U1;
+    float* U = rowfwd_x<MODE>(G, it);  // x0 of this IRLS iteration, or D in mode 2
+    const float* Lo = rowfwd_lo(G, it);
     const float* pk = (MODE == 2) ? G.p0 : nullptr;
     const float alpha = (MODE == 2) ? st->alpha : 0.f;
     double acc[2] = {0.0, 0.0};
@@ -112,8 +118,8 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowf_p2(const 
     __syncthreads();  // previous row pair's reads of sm are done
     for (int c4 = t; c4 < N / 4; c4 += T) {
         const int j = 4 * c4;
-        const float4 a = rowf_vals4<MODE>(G, U, pk, alpha, i0, j, acc);
-        const float4 b = has1 ? rowf_vals4<MODE>(G, U, pk, alpha, i1, j, acc) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 a = rowf_vals4<MODE>(G, U, Lo, pk, alpha, i0, j, acc);
+        const float4 b = has1 ? rowf_vals4<MODE>(G, U, Lo, pk, alpha, i1, j, acc) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int c = 0; c < 4; c++) sm[pad16(mk_pos(j + c, N))] = make_float2(f4get(a, c), f4get(b, c));
     }
@@ -354,9 +360,20 @@ static cudaError_t rowi_p2_n(int mode, int nblk, cudaStream_t s, const GridDev* 
     }
 }
 
-// column pairs per CTA: 512 threads (two pairs at N = 4096: 16-byte row segments)
+// column pairs per CTA: from N = 2048 up, UNW_COL_P2_THREADS threads (512: two pairs at
+// N = 4096, 16-byte row segments; at least one pair, at most eight); below, four pairs,
+// which gives short columns enough CTAs (measured on B200: at N = 1024, 18.8 us per launch
+// against 27.0 us with eight pairs; at N = 512, 13.7 us against 16.5 us)
+#ifndef UNW_COL_P2_THREADS
+#define UNW_COL_P2_THREADS 512
+#endif
 template <int N>
-constexpr int col_nseq_p2() { return N >= 8192 ? 1 : (8192 / N > 8 ? 8 : 8192 / N); }
+constexpr int col_nseq_p2() {
+    return N < 2048 ? 4
+                    : (UNW_COL_P2_THREADS / (N / 16) < 1
+                           ? 1
+                           : (UNW_COL_P2_THREADS / (N / 16) > 8 ? 8 : UNW_COL_P2_THREADS / (N / 16)));
+}
 
 template <int N>
 static cudaError_t col_p2_n(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* st, int n) {

@@ -14,7 +14,7 @@
 #define UNW_MAX_LOG 64       // per-IRLS-iteration CG counts kept in the state
 
 // Kernel shapes; each has its own CTA prefix array.
-enum { KS_ROWPAIR = 0, KS_COL = 1, KS_STEN = 2, KS_ELEM = 3, KS_ONE = 4, KS_MATVEC = 5, KS_NKIND = 6 };
+enum { KS_ROWPAIR = 0, KS_COL = 1, KS_STEN = 2, KS_ELEM = 3, KS_ONE = 4, KS_MATVEC = 5, KS_TC = 6, KS_NKIND = 7 };
 
 struct FftPlanDev {
     int n;                      // transform length
@@ -59,6 +59,7 @@ struct InstState {
     double residual;
     double best_residual;
     double rel_change;
+    double resid_rel;           // ||b - A u|| / ||b|| of the final system in float64 (k_resid)
     float tol, cg_tol, eps2;
     float cg_rel;               // > 0: cg_tol = cg_rel * ||r0|| at the PCG start
     int cg_max_iter;
@@ -91,7 +92,12 @@ struct GridDev {
     int sten_tiles_x;           // column tiles per stencil row strip
     float *gx, *gy, *wx, *wy;
     float *wIx, *wIy, *b, *r, *z, *p0, *p1, *Ap, *T;
+    // The IRLS iterate u is a float32 pair U + L with U = fl32(u) and |L| <= ulp(U)/2
+    // (about 48 significant bits): U0/L0 and U1/L1 ping-pong per IRLS iteration, Ub/Lb
+    // hold the best iterate.  The PCG accumulates its correction x - x0 in D (float32,
+    // zeroed at the PCG start); the IRLS tail adds it to the pair in float64.
     float *U0, *U1, *Ub;
+    float *L0, *L1, *Lb, *D;
     uint8_t* valid;
     // Neumann-Laplacian eigenvalue parts: lambda(k, j) = -(sH[k] + sW[j]) with
     // sH[k] = 4 sin^2(pi k / 2H), sW[j] = 4 sin^2(pi j / 2W), each computed in
@@ -204,6 +210,13 @@ __device__ __forceinline__ void finish_sum(const GridDev& G, int nctas, double (
     block_sum<NV>(v, sm);
     if (threadIdx.x == 0) *G.counter = 0u;
 }
+
+// Splits a float64 value into the float32 pair (hi, lo), hi = fl32(v), lo = fl32(v - hi).
+__device__ __forceinline__ void split_pair(double v, float& hi, float& lo) {
+    hi = __double2float_rn(v);
+    lo = isfinite(hi) ? __double2float_rn(v - (double)hi) : 0.f;
+}
+__device__ __forceinline__ double pair_val(float hi, float lo) { return (double)hi + (double)lo; }
 
 // Makhoul's even/odd reordering: x_n sits at position perm(n) of the sequence
 // whose DFT yields the DCT-II (J. Makhoul, IEEE TASSP 28(1), 1980).

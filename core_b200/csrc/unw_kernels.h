@@ -22,7 +22,8 @@ enum {
     UNW_K_INIT_RECENTRE,
     UNW_K_COPY_BEST,
     UNW_K_REL,
-    UNW_K_LAP_APPLY
+    UNW_K_LAP_APPLY,
+    UNW_K_RESID
 };
 
 // records the thread-local error text returned by unw_last_error(); returns code
@@ -58,6 +59,20 @@ cudaError_t unw_launch_rowi_bl(int M, int mode, int nblk, cudaStream_t s, const 
                                int n);
 cudaError_t unw_launch_col_bl(int M, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
                               int n);
+
+// tensor-core (tcgen05, split-precision bf16) column pass for grids of H <= UNW_TC_MAX_H rows
+#define UNW_TC_MAX_H 1024
+struct TcMaps {                       // four CUtensorMap (128 bytes each): C hi / lo, E hi / lo
+    alignas(64) unsigned char c_hi[128];
+    alignas(64) unsigned char c_lo[128];
+    alignas(64) unsigned char e_hi[128];
+    alignas(64) unsigned char e_lo[128];
+};
+size_t unw_tc_table_bytes(int H);     // workspace bytes of the split DCT matrices (0 if H > UNW_TC_MAX_H)
+int unw_tc_ctas(int H, int W);        // CTAs of one grid's tensor-core column pass
+cudaError_t unw_tc_prepare(int H, void* tab, TcMaps* maps, cudaStream_t s);
+cudaError_t unw_launch_col_tc(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts, int n,
+                              const TcMaps* maps);
 
 // bounding box of valid pixels on the caller's full grid
 cudaError_t unw_launch_bbox(const float* phase, long long pitch, int H0, int W0, int* rowany,

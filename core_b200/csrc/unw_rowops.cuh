@@ -19,10 +19,35 @@ __device__ __forceinline__ float lap_at(const float* __restrict__ x, const float
     return -res;
 }
 
+// Difference a - b of two iterate values held as float32 pairs.  fl(ah - bh) carries a
+// rounding error relative to the difference itself (not to |u|), and the low parts add
+// back what the storage of u in float32 would lose, so the result equals the exact
+// difference to a few float32 ulps of the difference.
+__device__ __forceinline__ float pair_diff(float ah, float al, float bh, float bl) {
+    return fadd(fsub(ah, bh), fsub(al, bl));
+}
+
+// A x at (i, j) for the iterate x = U + L held as a float32 pair: the reference's op
+// order (lap_at), each neighbour difference formed from the pair by pair_diff.
+__device__ __forceinline__ float lap_at_pair(const float* __restrict__ U, const float* __restrict__ L,
+                                             const float* __restrict__ wx, const float* __restrict__ wy, int i, int j,
+                                             int H, int W, int P) {
+    const size_t o = (size_t)i * P + j;
+    const float uc = U[o], lc = L[o];
+    float res = 0.f;
+    if (j > 0) res = fsub(res, fmul(pair_diff(uc, lc, U[o - 1], L[o - 1]), wx[o - 1]));
+    if (j < W - 1) res = fadd(res, fmul(pair_diff(U[o + 1], L[o + 1], uc, lc), wx[o]));
+    if (i > 0) res = fsub(res, fmul(pair_diff(uc, lc, U[o - P], L[o - P]), wy[o - P]));
+    if (i < H - 1) res = fadd(res, fmul(pair_diff(U[o + P], L[o + P], uc, lc), wy[o]));
+    return -res;
+}
+
 // Row-forward modes:
 //  0 RHO  rho = -div(w g), the DCT initial solve (utils_unwrap2d.py:1478-1483)
-//  1 R0   r = b - A x0, PCG start (utils_unwrap2d.py:1413-1419)
-//  2 UPD  x += alpha p; r -= alpha Ap (utils_unwrap2d.py:1445-1459)
+//  1 R0   r = b - A x0, PCG start (utils_unwrap2d.py:1413-1419), with the neighbour
+//         differences of x0 formed from the iterate pair; D (the PCG correction) = 0
+//  2 UPD  x += alpha p; r -= alpha Ap (utils_unwrap2d.py:1445-1459); x is the
+//         correction D = x - x0, added to the iterate pair at the IRLS tail
 //  3 COPY r as given (operator entry point)
 template <int MODE>
 __device__ __forceinline__ bool rowfwd_gate(const InstState* s) {
@@ -31,9 +56,18 @@ __device__ __forceinline__ bool rowfwd_gate(const InstState* s) {
     return s->irls_active != 0 && s->cg_active != 0;
 }
 
+// The iterate pointers of a row-forward pass at IRLS iteration `it`: mode 1 reads the
+// current pair (U, L); mode 2 updates D.
 template <int MODE>
-__device__ __forceinline__ float rowfwd_value(const GridDev& G, float* __restrict__ U, const float* __restrict__ pk,
-                                              float alpha, int i, int j, double (&acc)[2]) {
+__device__ __forceinline__ float* rowfwd_x(const GridDev& G, int it) {
+    return MODE == 2 ? G.D : ((it & 1) ? G.U0 : G.U1);
+}
+__device__ __forceinline__ const float* rowfwd_lo(const GridDev& G, int it) { return (it & 1) ? G.L0 : G.L1; }
+
+template <int MODE>
+__device__ __forceinline__ float rowfwd_value(const GridDev& G, float* __restrict__ U, const float* __restrict__ Lo,
+                                              const float* __restrict__ pk, float alpha, int i, int j,
+                                              double (&acc)[2]) {
     const int H = G.H, W = G.W, P = G.P;
     const size_t o = (size_t)i * P + j;
     if (MODE == 0) {
@@ -46,9 +80,10 @@ __device__ __forceinline__ float rowfwd_value(const GridDev& G, float* __restric
     } else if (MODE == 3) {
         return G.r[o];
     } else if (MODE == 1) {
-        const float ax = lap_at(U, G.wIx, G.wIy, i, j, H, W, P);
+        const float ax = lap_at_pair(U, Lo, G.wIx, G.wIy, i, j, H, W, P);
         const float val = fsub(G.b[o], ax);
         G.r[o] = val;
+        G.D[o] = 0.f;
         acc[0] += isfinite(val) ? 0.0 : 1.0;
         acc[1] += (double)val * (double)val;
         return val;

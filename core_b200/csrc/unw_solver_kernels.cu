@@ -77,7 +77,7 @@ __global__ void k_state_init(const GridDev* __restrict__ grids, int n, UnwScalar
     s->cg_active = 0; s->cg_iter = 0;
     s->irls_active = sc.max_iter > 0; s->irls_iter = 0; s->max_iter = sc.max_iter;
     s->best_update = 0; s->revert = 0; s->u_index = 0; s->status = 0;
-    s->vcount = 0; s->mean = 0; s->residual = 0; s->best_residual = INFINITY; s->rel_change = 0;
+    s->vcount = 0; s->mean = 0; s->residual = 0; s->best_residual = INFINITY; s->rel_change = 0; s->resid_rel = 0;
     s->tol = sc.tol; s->cg_tol = sc.cg_tol; s->eps2 = sc.eps2; s->cg_max_iter = sc.cg_max_iter;
     s->cg_rel = sc.cg_rel;
     s->cg_total = 0;
@@ -158,7 +158,8 @@ __global__ void __launch_bounds__(T) k_row_fwd(const GridDev* __restrict__ grids
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
     double acc[2] = {0.0, 0.0};
-    float* U = (it & 1) ? G.U0 : G.U1;  // x of this IRLS iteration (U_nxt)
+    float* U = rowfwd_x<MODE>(G, it);  // x0 of this IRLS iteration (U_nxt), or D in mode 2
+    const float* Lo = rowfwd_lo(G, it);
     const float* pk = (MODE == 2) ? G.p0 : nullptr;
     const float alpha = (MODE == 2) ? st->alpha : 0.f;
     for (int pair = local; pair < (H + 1) / 2; pair += nct) {
@@ -166,8 +167,8 @@ __global__ void __launch_bounds__(T) k_row_fwd(const GridDev* __restrict__ grids
     const bool has1 = i1 < H;
     __syncthreads();  // previous row pair's reads of sm are done
     for (int j = threadIdx.x; j < W; j += T) {
-        const float a = rowfwd_value<MODE>(G, U, pk, alpha, i0, j, acc);
-        const float b = has1 ? rowfwd_value<MODE>(G, U, pk, alpha, i1, j, acc) : 0.f;
+        const float a = rowfwd_value<MODE>(G, U, Lo, pk, alpha, i0, j, acc);
+        const float b = has1 ? rowfwd_value<MODE>(G, U, Lo, pk, alpha, i1, j, acc) : 0.f;
         sm[mk_perm(j, W)] = make_float2(a, b);
     }
     __syncthreads();
@@ -444,11 +445,15 @@ __global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ g
 }
 
 // IRLS head (utils_unwrap2d.py:1536-1581): recentre, residual gradients,
-// best-iterate test, IRLS weights and right-hand side.  Reads U_cur, writes
-// the recentred iterate to U_nxt (U_cur keeps u_prev for the convergence test).
+// best-iterate test, IRLS weights and right-hand side.  Reads the iterate pair
+// (U_cur, L_cur), writes the recentred pair to (U_nxt, L_nxt) (the current pair
+// keeps u_prev for the convergence test).  The residual gradients take the
+// neighbour differences of the pair (pair_diff; the mean cancels in them), the
+// recentred pair is formed in float64, the weights and b are float32 in the
+// reference's op order.
 // One warp per row, 4 columns per lane; the weight of the left edge comes from
 // the neighbouring lane, the weight of the upper edge is recomputed from the
-// row above (the same float32 operations, so it equals that row's own value).
+// row above (the same operations, so it equals that row's own value).
 __device__ __forceinline__ float irls_w(float w, float r, float eps2) {
     return clampf_nan(fdiv(w, __fsqrt_rn(fadd(fmul(r, r), eps2))), 1e-6f, 1e6f);
 }
@@ -466,10 +471,12 @@ __global__ void __launch_bounds__(256, 4) k_head(const GridDev* __restrict__ gri
     const int nct = starts[g + 1] - starts[g];
     const int H = G.H, W = G.W, P = G.P;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const float m = st->vcount > 0 ? (float)st->mean : 0.f;
+    const double m = st->vcount > 0 ? st->mean : 0.0;
     const float eps2 = st->eps2;
     const float* __restrict__ uc = (it & 1) ? G.U1 : G.U0;
+    const float* __restrict__ lc = (it & 1) ? G.L1 : G.L0;
     float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
+    float* __restrict__ ln = (it & 1) ? G.L0 : G.L1;
     double acc[2] = {0.0, 0.0};
     const int ntiles = G.sten_tiles_x * ((H + 8 * G.sten_rows - 1) / (8 * G.sten_rows));
     for (int tile = local; tile < ntiles; tile += nct) {
@@ -479,39 +486,40 @@ __global__ void __launch_bounds__(256, 4) k_head(const GridDev* __restrict__ gri
     const bool on = i < H && j0 < W;
     const bool hu = i > 0, hd = i < H - 1;
     const size_t o = (size_t)i * P + j0;
-    F4 u{}, ud{}, uu{}, gx{}, gy{}, gyu{}, wx{}, wy{}, wyu{};
-    float ul = 0.f, ur = 0.f, gxl = 0.f, wxl = 0.f;
+    F4 u{}, l{}, ud{}, ld{}, uu{}, lu{}, gx{}, gy{}, gyu{}, wx{}, wy{}, wyu{};
+    float ul = 0.f, ll = 0.f, ur = 0.f, lr = 0.f, gxl = 0.f, wxl = 0.f;
     if (on) {
         u = ld4(uc, o);
-        if (hd) ud = ld4(uc, o + P);
-        if (hu) { uu = ld4(uc, o - P); gyu = ld4(G.gy, o - P); wyu = ld4(G.wy, o - P); }
+        l = ld4(lc, o);
+        if (hd) { ud = ld4(uc, o + P); ld = ld4(lc, o + P); }
+        if (hu) { uu = ld4(uc, o - P); lu = ld4(lc, o - P); gyu = ld4(G.gy, o - P); wyu = ld4(G.wy, o - P); }
         gx = ld4(G.gx, o);
         gy = ld4(G.gy, o);
         wx = ld4(G.wx, o);
         wy = ld4(G.wy, o);
-        if (lane == 0 && j0 > 0) { ul = uc[o - 1]; gxl = G.gx[o - 1]; wxl = G.wx[o - 1]; }
-        if (lane == 31 && j0 + 4 < W) ur = uc[o + 4];
+        if (lane == 0 && j0 > 0) { ul = uc[o - 1]; ll = lc[o - 1]; gxl = G.gx[o - 1]; wxl = G.wx[o - 1]; }
+        if (lane == 31 && j0 + 4 < W) { ur = uc[o + 4]; lr = lc[o + 4]; }
     }
-    F4 c, rx, ry, wix, wiy, bv;
-#pragma unroll
-    for (int q = 0; q < 4; q++) c.v[q] = fsub(u.v[q], m);
-    // right neighbour of column j0+3 and left neighbour of j0 (recentred)
-    float cr = __shfl_down_sync(0xffffffffu, c.v[0], 1);
-    if (lane == 31) cr = fsub(ur, m);
+    float rx[4], ry[4];
+    F4 wix, wiy, bv;
+    // right neighbour of column j0+3
+    float urh = __shfl_down_sync(0xffffffffu, u.v[0], 1);
+    float url = __shfl_down_sync(0xffffffffu, l.v[0], 1);
+    if (lane == 31) { urh = ur; url = lr; }
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const int j = j0 + q;
-        const float right = q == 3 ? cr : c.v[q + 1];
+        const float rh = q == 3 ? urh : u.v[q + 1], rl = q == 3 ? url : l.v[q + 1];
         // r = grad(u) - g, last column / row: 0 - g
-        rx.v[q] = (j < W - 1) ? fsub(fsub(right, c.v[q]), gx.v[q]) : fsub(0.f, gx.v[q]);
-        ry.v[q] = hd ? fsub(fsub(fsub(ud.v[q], m), c.v[q]), gy.v[q]) : fsub(0.f, gy.v[q]);
-        wix.v[q] = irls_w(wx.v[q], rx.v[q], eps2);
-        wiy.v[q] = irls_w(wy.v[q], ry.v[q], eps2);
+        rx[q] = (j < W - 1) ? fsub(pair_diff(rh, rl, u.v[q], l.v[q]), gx.v[q]) : fsub(0.f, gx.v[q]);
+        ry[q] = hd ? fsub(pair_diff(ud.v[q], ld.v[q], u.v[q], l.v[q]), gy.v[q]) : fsub(0.f, gy.v[q]);
+        wix.v[q] = irls_w(wx.v[q], rx[q], eps2);
+        wiy.v[q] = irls_w(wy.v[q], ry[q], eps2);
     }
     float wl = __shfl_up_sync(0xffffffffu, wix.v[3], 1);
     float gl = __shfl_up_sync(0xffffffffu, gx.v[3], 1);
     if (lane == 0 && j0 > 0) {
-        const float rxl = fsub(fsub(c.v[0], fsub(ul, m)), gxl);
+        const float rxl = fsub(pair_diff(u.v[0], l.v[0], ul, ll), gxl);
         wl = irls_w(wxl, rxl, eps2);
         gl = gxl;
     }
@@ -526,18 +534,25 @@ __global__ void __launch_bounds__(256, 4) k_head(const GridDev* __restrict__ gri
         }
         if (j < W - 1) b = fsub(b, fmul(wix.v[q], gx.v[q]));
         if (hu) {
-            const float ryu = fsub(fsub(c.v[q], fsub(uu.v[q], m)), gyu.v[q]);
+            const float ryu = fsub(pair_diff(u.v[q], l.v[q], uu.v[q], lu.v[q]), gyu.v[q]);
             b = fadd(b, fmul(irls_w(wyu.v[q], ryu, eps2), gyu.v[q]));
         }
         if (hd) b = fsub(b, fmul(wiy.v[q], gy.v[q]));
         bv.v[q] = b;
-        if (on && j < W) {
-            acc[0] += (double)fmul(rx.v[q], rx.v[q]) + (double)fmul(ry.v[q], ry.v[q]);
-            acc[1] += isfinite(c.v[q]) ? 0.0 : 1.0;
-        }
     }
     if (on) {
-        st4(un, o, c);
+        F4 ch, cl4;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const double c = pair_val(u.v[q], l.v[q]) - m;
+            split_pair(c, ch.v[q], cl4.v[q]);
+            if (j0 + q < W) {
+                acc[0] += (double)fmul(rx[q], rx[q]) + (double)fmul(ry[q], ry[q]);
+                acc[1] += isfinite(c) ? 0.0 : 1.0;
+            }
+        }
+        st4(un, o, ch);
+        st4(ln, o, cl4);
         st4(G.wIx, o, wix);
         st4(G.wIy, o, wiy);
         st4(G.b, o, bv);
@@ -566,7 +581,7 @@ __global__ void __launch_bounds__(256, 4) k_head(const GridDev* __restrict__ gri
     for (int i = (local); i < (G).H; i += (nct))              \
         for (int j = 4 * threadIdx.x; j < (G).W; j += 4 * blockDim.x)
 
-// sum over all pixels of u * valid (utils_unwrap2d.py:1539-1541)
+// sum over all pixels of u * valid (utils_unwrap2d.py:1539-1541), u = U + L in float64
 __global__ void k_mean(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n, int it) {
     __shared__ double red[32 * 1];
     const int g = find_grid(starts, n, blockIdx.x);
@@ -576,15 +591,16 @@ __global__ void k_mean(const GridDev* __restrict__ grids, const int* __restrict_
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const float* __restrict__ uc = (it & 1) ? G.U1 : G.U0;
+    const float* __restrict__ lc = (it & 1) ? G.L1 : G.L0;
     double acc[1] = {0.0};
     UNW_ROWS_LOOP(G, local, nct) {
         const size_t o = (size_t)i * G.P + j;
-        const F4 u = ld4(uc, o);
+        const F4 u = ld4(uc, o), l = ld4(lc, o);
         const uchar4 v = *reinterpret_cast<const uchar4*>(G.valid + o);
         const unsigned char vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int q = 0; q < 4; q++)
-            if (j + q < G.W) acc[0] += (double)(u.v[q] * (vv[q] ? 1.f : 0.f));
+            if (j + q < G.W) acc[0] += pair_val(u.v[q], l.v[q]) * (vv[q] ? 1.0 : 0.0);
     }
     if (arrive<1>(G, local, nct, acc, red)) {
         finish_sum<1>(G, nct, acc, red);
@@ -592,21 +608,25 @@ __global__ void k_mean(const GridDev* __restrict__ grids, const int* __restrict_
     }
 }
 
-// After the DCT initial solve: u -= mean_valid(u); u_best = u (utils_unwrap2d.py:1509-1531).
+// After the DCT initial solve: u -= mean_valid(u); u_best = u (utils_unwrap2d.py:1509-1531),
+// in float64 into the iterate pair (U0, L0) and the best pair (Ub, Lb).
 __global__ void k_init_recentre(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
     const int g = find_grid(starts, n, blockIdx.x);
     const GridDev& G = grids[g];
     const InstState* st = G.st;
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
-    const float m = st->vcount > 0 ? (float)st->mean : 0.f;
+    const double m = st->vcount > 0 ? st->mean : 0.0;
     UNW_ROWS_LOOP(G, local, nct) {
         const size_t o = (size_t)i * G.P + j;
-        F4 u = ld4(G.U0, o);
+        const F4 u = ld4(G.U0, o);
+        F4 hi, lo;
 #pragma unroll
-        for (int q = 0; q < 4; q++) u.v[q] = fsub(u.v[q], m);
-        st4(G.U0, o, u);
-        st4(G.Ub, o, u);
+        for (int q = 0; q < 4; q++) split_pair((double)u.v[q] - m, hi.v[q], lo.v[q]);
+        st4(G.U0, o, hi);
+        st4(G.L0, o, lo);
+        st4(G.Ub, o, hi);
+        st4(G.Lb, o, lo);
     }
 }
 
@@ -619,14 +639,17 @@ __global__ void k_copy_best(const GridDev* __restrict__ grids, const int* __rest
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
+    const float* __restrict__ ln = (it & 1) ? G.L0 : G.L1;
     UNW_ROWS_LOOP(G, local, nct) {
         const size_t o = (size_t)i * G.P + j;
         st4(G.Ub, o, ld4(un, o));
+        st4(G.Lb, o, ld4(ln, o));
     }
 }
 
-// IRLS tail (utils_unwrap2d.py:1599-1626): non-finite -> revert to u_best and
-// stop; rel_change = |u_prev - u| / (|u| + 1e-10) over the full grid.
+// IRLS tail (utils_unwrap2d.py:1599-1626): u = x0 + D (the PCG result, formed in
+// float64 into the iterate pair); non-finite -> revert to u_best and stop;
+// rel_change = |u_prev - u| / (|u| + 1e-10) over the full grid.
 __global__ void k_rel(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n, int it) {
     __shared__ double red[32 * 3];
     const int g = find_grid(starts, n, blockIdx.x);
@@ -636,19 +659,26 @@ __global__ void k_rel(const GridDev* __restrict__ grids, const int* __restrict__
     const int local = blockIdx.x - starts[g];
     const int nct = starts[g + 1] - starts[g];
     const float* __restrict__ up = (it & 1) ? G.U1 : G.U0;
-    const float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
+    const float* __restrict__ lp = (it & 1) ? G.L1 : G.L0;
+    float* __restrict__ un = (it & 1) ? G.U0 : G.U1;
+    float* __restrict__ ln = (it & 1) ? G.L0 : G.L1;
     double acc[3] = {0.0, 0.0, 0.0};
     UNW_ROWS_LOOP(G, local, nct) {
         const size_t o = (size_t)i * G.P + j;
-        const F4 u = ld4(un, o), v = ld4(up, o);
+        const F4 uh = ld4(un, o), ul = ld4(ln, o), dd = ld4(G.D, o), vh = ld4(up, o), vl = ld4(lp, o);
+        F4 nh, nl;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            if (j + q >= G.W) break;
-            const float d = fsub(v.v[q], u.v[q]);
-            acc[0] += (double)d * (double)d;
-            acc[1] += (double)u.v[q] * (double)u.v[q];
-            acc[2] += isfinite(u.v[q]) ? 0.0 : 1.0;
+            const double u = pair_val(uh.v[q], ul.v[q]) + (double)dd.v[q];
+            split_pair(u, nh.v[q], nl.v[q]);
+            if (j + q >= G.W) continue;
+            const double d = pair_val(vh.v[q], vl.v[q]) - u;
+            acc[0] += d * d;
+            acc[1] += u * u;
+            acc[2] += isfinite(u) ? 0.0 : 1.0;
         }
+        st4(un, o, nh);
+        st4(ln, o, nl);
     }
     if (arrive<3>(G, local, nct, acc, red)) {
         finish_sum<3>(G, nct, acc, red);
@@ -668,6 +698,35 @@ __global__ void k_rel(const GridDev* __restrict__ grids, const int* __restrict__
                 if (rel < (double)st->tol || st->irls_iter >= st->max_iter) st->irls_active = 0;
             }
         }
+    }
+}
+
+// ||b - A u|| / ||b|| in float64 for the final iterate pair (u_index) and the weights
+// and right-hand side of the last IRLS head: how far the result is from an exact
+// solve of the last weighted Poisson system (utils_unwrap2d.py:1576-1593).
+__global__ void k_resid(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
+    __shared__ double red[32 * 2];
+    const int g = find_grid(starts, n, blockIdx.x);
+    const GridDev& G = grids[g];
+    InstState* st = G.st;
+    if (st->irls_iter == 0) return;
+    const int local = blockIdx.x - starts[g];
+    const int nct = starts[g + 1] - starts[g];
+    const int H = G.H, W = G.W, P = G.P;
+    const float* U = st->u_index == 2 ? G.Ub : (st->u_index == 1 ? G.U1 : G.U0);
+    const float* L = st->u_index == 2 ? G.Lb : (st->u_index == 1 ? G.L1 : G.L0);
+    const long long npx = (long long)H * W;
+    double acc[2] = {0.0, 0.0};
+    for (long long q = (long long)local * blockDim.x + threadIdx.x; q < npx; q += (long long)nct * blockDim.x) {
+        const int i = (int)(q / W), j = (int)(q - (long long)i * W);
+        const double b = (double)G.b[(size_t)i * P + j];
+        const double r = b - lap_at_pair(U, L, G.wIx, G.wIy, i, j, H, W, P);
+        acc[0] += r * r;
+        acc[1] += b * b;
+    }
+    if (arrive<2>(G, local, nct, acc, red)) {
+        finish_sum<2>(G, nct, acc, red);
+        if (threadIdx.x == 0) st->resid_rel = acc[1] > 0.0 ? sqrt(acc[0] / acc[1]) : sqrt(acc[0]);
     }
 }
 
@@ -803,6 +862,7 @@ cudaError_t unw_launch_simple(int which, int nblk, cudaStream_t s, const GridDev
         case UNW_K_COPY_BEST: k_copy_best<<<nblk, 256, 0, s>>>(gd, starts, n, it); break;
         case UNW_K_REL: k_rel<<<nblk, 256, 0, s>>>(gd, starts, n, it); break;
         case UNW_K_LAP_APPLY: k_lap_apply<<<nblk, 256, 0, s>>>(gd, starts, n); break;
+        case UNW_K_RESID: k_resid<<<nblk, 256, 0, s>>>(gd, starts, n); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -72,8 +72,32 @@ def resolve_device(device, phase=None):
     return dev
 
 
+PRECISIONS = ("plain", "mixed")
+COL_PASSES = ("auto", "tc", "fft")
+
+
+def precision_flags(precision="plain", col_pass="auto"):
+    """UNW_F_* bits of the precision keywords.
+
+    precision='plain'  float32 FFT DCTs throughout (the reference's arithmetic);
+    precision='mixed'  for grids of at most 1024 rows the column DCT / scaling /
+                       inverse DCT of the preconditioner may run as split-precision
+                       bf16 products on the tensor cores: col_pass='auto' lets the
+                       autotuner time both on the first call for a shape, 'tc' / 'fft'
+                       force one; the stats report the path and the float64 residual of
+                       the final weighted system.
+    """
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {PRECISIONS}, got {precision!r}")
+    if col_pass not in COL_PASSES:
+        raise ValueError(f"col_pass must be one of {COL_PASSES}, got {col_pass!r}")
+    if precision == "plain":
+        return 0
+    return _lib.UNW_F_MIXED | {"auto": 0, "tc": _lib.UNW_F_COL_TC, "fft": _lib.UNW_F_COL_FFT}[col_pass]
+
+
 def make_params(max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2, conncomp_size=30,
-                congruent=False, check_every=1, fixed_iters=False):
+                congruent=False, check_every=1, fixed_iters=False, precision="plain", col_pass="auto"):
     p = _lib.UnwParams()
     p.max_iter = int(max_iter)
     p.tol = float(tol)
@@ -81,7 +105,8 @@ def make_params(max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2
     p.cg_tol = float(cg_tol)
     p.epsilon = float(epsilon)
     p.conncomp_size = int(conncomp_size)
-    p.flags = (_lib.UNW_F_CONGRUENT if congruent else 0) | (_lib.UNW_F_FIXED_ITERS if fixed_iters else 0)
+    p.flags = ((_lib.UNW_F_CONGRUENT if congruent else 0) | (_lib.UNW_F_FIXED_ITERS if fixed_iters else 0)
+               | precision_flags(precision, col_pass))
     p.check_every = int(check_every)
     return p
 
@@ -144,7 +169,8 @@ def _ws():
 
 def irls_unwrap_2d(phase, weight=None, device='auto', max_iter=50, tol=1e-3,
                    cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2, conncomp_size=30, debug=False,
-                   *, congruent=False, return_stats=False, check_every=1, fixed_iters=False):
+                   *, congruent=False, return_stats=False, check_every=1, fixed_iters=False,
+                   precision="plain", col_pass="auto"):
     """Unwrap 2-D phase with the DCT-preconditioned IRLS L1 solver on a B200.
 
     Same parameters and outputs as the reference (utils_unwrap2d.py:1082-1083).
@@ -154,6 +180,9 @@ def irls_unwrap_2d(phase, weight=None, device='auto', max_iter=50, tol=1e-3,
       check_every   IRLS iterations enqueued between device->host convergence reads
       fixed_iters   run exactly max_iter x cg_max_iter iterations (tol / cg_tol stop
                     tests off, numerical breaks kept): identical work for timing
+      precision     'plain' (float32 FFT DCTs) or 'mixed' (tensor-core column pass for
+                    grids of <= 1024 rows where the autotuner finds it faster)
+      col_pass      with precision='mixed': 'auto', or force 'tc' / 'fft'
     """
     torch = _torch()
     is_torch = isinstance(phase, torch.Tensor)
@@ -173,7 +202,7 @@ def irls_unwrap_2d(phase, weight=None, device='auto', max_iter=50, tol=1e-3,
         ws = _ws().get(dev, nbytes)
         st = _lib.UnwStats()
         prm = make_params(max_iter, tol, cg_max_iter, cg_tol, epsilon, conncomp_size, congruent, check_every,
-                          fixed_iters)
+                          fixed_iters, precision, col_pass)
         stream = torch.cuda.current_stream(dev).cuda_stream
         rc = lib.unw_solve_f32(ph.data_ptr(), W, wt.data_ptr() if wt is not None else None, W, H, W,
                                C.byref(prm), out_u.data_ptr(), W, out_cc.data_ptr(), W,
@@ -202,7 +231,8 @@ def irls_unwrap_2d(phase, weight=None, device='auto', max_iter=50, tol=1e-3,
 
 def irls_unwrap_2d_batch(phases, weights=None, device='auto', max_iter=50, tol=1e-3, cg_max_iter=20,
                          cg_tol=1e-4, epsilon=1e-2, conncomp_size=30, debug=False, *, congruent=False,
-                         return_stats=False, check_every=1, fixed_iters=False):
+                         return_stats=False, check_every=1, fixed_iters=False, precision="plain",
+                         col_pass="auto"):
     """Unwrap a list of independent grids (any sizes) in one batched launch sequence.
 
     Each grid converges on its own test, exactly as if `irls_unwrap_2d` had been
@@ -251,7 +281,7 @@ def irls_unwrap_2d_batch(phases, weights=None, device='auto', max_iter=50, tol=1
         ws = _ws().get(dev, nbytes)
         sts = (_lib.UnwStats * n)()
         prm = make_params(max_iter, tol, cg_max_iter, cg_tol, epsilon, conncomp_size, congruent, check_every,
-                          fixed_iters)
+                          fixed_iters, precision, col_pass)
         rc = lib.unw_solve_batch(n, grids, C.byref(prm), ws.data_ptr(), ws.numel(), sts,
                                  torch.cuda.current_stream(dev).cuda_stream)
         _lib.check(rc, "unw_solve_batch")

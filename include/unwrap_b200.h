@@ -29,7 +29,7 @@ extern "C" {
 #define UNW_API
 #endif
 
-#define UNW_ABI_VERSION 1
+#define UNW_ABI_VERSION 2
 
 enum {
     UNW_OK = 0,
@@ -60,6 +60,15 @@ typedef struct unw_params {
 #define UNW_F_FIXED_ITERS 8 /* run max_iter IRLS x cg_max_iter PCG iterations: the tol and
                                cg_tol stop tests are off, the numerical breaks stay (for
                                comparing throughput at identical work)                      */
+#define UNW_F_MIXED 16      /* mixed-precision form: for grids of at most 1024 rows the column
+                               DCT / scaling / inverse DCT of the preconditioner may run as
+                               split-precision bf16 products on the tensor cores, where an
+                               autotuner (timing both on the first call for a shape) finds
+                               them faster than the float32 FFT pass; unw_stats reports the
+                               choice and the float64 residual of the final system         */
+#define UNW_F_COL_TC 32     /* with UNW_F_MIXED: always the tensor-core column pass (else
+                               UNW_E_UNSUPPORTED), no autotuning                             */
+#define UNW_F_COL_FFT 64    /* with UNW_F_MIXED: always the float32 FFT column pass          */
 
 /* Kernel families timed under UNW_F_PROFILE (index into unw_stats.prof_*). */
 enum {
@@ -83,12 +92,22 @@ typedef struct unw_stats {
     int32_t cg_iters[64];   /* PCG iterations of the first 64 IRLS iterations    */
     float prof_ms[16];      /* summed kernel time per family (UNW_F_PROFILE)     */
     int32_t prof_launches[16]; /* launches per family (UNW_F_PROFILE)            */
+    int32_t col_path;       /* column pass used: 0 float32 FFT, 1 tensor cores  */
+    float tune_ms[2];       /* autotuner: FFT / tensor-core column pass, ms per
+                               launch (UNW_F_MIXED, 0 when not timed)          */
+    int32_t pad_;
+    double resid_rel;       /* ||b - A u|| / ||b|| of the final weighted system
+                               in float64 (UNW_F_MIXED; 0 otherwise): the error
+                               of the result against an exact solve of the last
+                               IRLS system                                     */
 } unw_stats;
 
 #define UNW_S_DCT_INIT_NONFINITE 1   /* DCT init produced NaN/inf (zero-filled)  */
 #define UNW_S_REVERTED           2   /* reverted to the best iterate             */
 #define UNW_S_NONFINITE_OUT      4   /* non-finite output: NaN result            */
 #define UNW_S_ALL_NAN            8   /* input all NaN                            */
+#define UNW_S_TC_TIMEOUT        16   /* a tensor-core pass gave up waiting on its
+                                        pipeline (bounded wait); result not valid */
 
 /* One grid of a batched solve (unw_solve_batch).  Pitches are in elements. */
 typedef struct unw_grid {
@@ -156,6 +175,15 @@ UNW_API int unw_apply_laplacian(const float* x, const float* wx, const float* wy
  * utils_unwrap2d.py:1390-1403 (also the DCT initial solve :1478-1513). */
 UNW_API int unw_apply_preconditioner(const float* r, int64_t H, int64_t W, float* z,
                              void* workspace, size_t workspace_bytes, void* cuda_stream);
+
+/* The same operator in the mixed-precision form: col_path 1 runs the column
+ * DCT / scaling / inverse DCT as split-precision bf16 products on the tensor
+ * cores (H <= 1024 and W a multiple of 4, else UNW_E_UNSUPPORTED), 0 the float32
+ * FFT pass, -1 lets the autotuner choose.  Returns the path used (0 or 1) or a
+ * negative error code.  It has no counterpart in the reference (which has one
+ * float32 DCT path, utils_unwrap2d.py:1316-1365). */
+UNW_API int unw_apply_preconditioner_mixed(const float* r, int64_t H, int64_t W, float* z, int32_t col_path,
+                                           void* workspace, size_t workspace_bytes, void* cuda_stream);
 
 /*
  * Gradients through the unwrap (frozen-weight implicit adjoint).  It has no

@@ -15,6 +15,9 @@ An FP64 variant of the same function is made by substituting only the two dtype
 lines (`dtype = torch.float32`, `np_dtype = np.float32`, :1192-1193) in a scratch
 copy of the module.
 
+`--stack` runs members 0-2 of the 64-grid uneven stack (rows 1500-2600, cols
+4000-7000, gen_stack_meta(64, 0)).
+
 Outputs: small `.npz` fixtures next to this script holding inputs, parameters,
 the reference's (unwrapped, conncomp) and its IRLS iteration count.  Grids of
 1024^2 and above store the full 2-pi cycle map (int16) plus the unwrapped phase
@@ -168,14 +171,16 @@ def save_full(name, phase, weight, params, u, cc, iters, secs, precision):
         precision=np.array(precision), seconds=np.array(secs))
 
 
-def save_large(name, gen, gen_args, params, phase, u, cc, iters, secs, precision, step):
-    """Large grids: regenerate inputs from (gen, gen_args); store cycle map + sub-sampled u."""
+def save_large(name, gen, gen_args, params, phase, u, cc, iters, secs, precision, step, cycles=True):
+    """Large grids: regenerate inputs from (gen, gen_args); store cycle map + sub-sampled u
+    (without the cycle map when `cycles` is false)."""
     v = np.isfinite(phase) & np.isfinite(u)
     k = np.zeros(phase.shape, np.int16)
     k[v] = np.round((u[v].astype(np.float64) - phase[v].astype(np.float64)) / (2 * np.pi)).astype(np.int16)
+    extra = dict(cycles=k) if cycles else {}
     np.savez_compressed(
         os.path.join(HERE, f"{name}.npz"), gen=np.array(gen), gen_args=np.array(gen_args, dtype=np.int64),
-        cycles=k, step=np.array(step), u_sub=u[::step, ::step], cc_sub=cc[::step, ::step],
+        step=np.array(step), u_sub=u[::step, ::step], cc_sub=cc[::step, ::step], **extra,
         cc_hist=np.bincount(cc.ravel().astype(np.int64)), iters=np.array(iters),
         params=np.array([params[k2] for k2 in ("max_iter", "tol", "cg_max_iter", "cg_tol", "epsilon", "conncomp_size")],
                         dtype=np.float64),
@@ -190,6 +195,9 @@ def main():
     ap.add_argument("--xlarge", action="store_true", help="also the 4096^2 fault grid (~8 min)")
     ap.add_argument("--xlarge64", action="store_true",
                     help="FP64 runs at full size: the 4096^2 fault grid and the G1 grid at 2048^2 and 4096^2")
+    ap.add_argument("--stack", action="store_true",
+                    help="members 0, 1, 2 of the 64-grid uneven stack (gen_stack_meta(64, 0)): FP32 run "
+                         "(cycle map + lattice) and FP64 run (lattice)")
     ap.add_argument("--only", default=None)
     ap.add_argument("--no-small", action="store_true", help="skip the small fixtures")
     a = ap.parse_args()
@@ -219,6 +227,8 @@ def main():
         u, cc, it, s = run_ref(f32, p, c, FN_DEFAULTS)
         save_large("L_g2_4096_fn_fp32", "g2", (4096, 4096, 0), FN_DEFAULTS, p, u, cc, it, s, "fp32", 16)
         print(f"L_g2_4096_fn_fp32: iters={it} {s:.2f}s")
+    if a.stack:
+        stack_fixtures(f32, f64)
     if a.xlarge64:
         for name, gen, args, step in (("L_g1_2048_fn_fp64", "g1", (2048, 2048, 0), 8),
                                       ("L_g2_4096_fn_fp64", "g2", (4096, 4096, 0), 16),
@@ -229,6 +239,18 @@ def main():
             u, cc, it, s = run_ref(f64, p, c, FN_DEFAULTS)
             save_large(name, gen, args, FN_DEFAULTS, p, u, cc, it, s, "fp64", step)
             print(f"{name}: iters={it} {s:.2f}s", flush=True)
+
+
+def stack_fixtures(f32, f64):
+    from core_b200.synthetic import gen_stack_grid, gen_stack_meta
+    meta = gen_stack_meta(64, seed=0)
+    for m in (0, 1, 2):
+        p, c, _ = gen_stack_grid(meta[m])
+        for prec, fn in (("fp32", f32), ("fp64", f64)):
+            u, cc, it, s = run_ref(fn, p, c, FN_DEFAULTS)
+            save_large(f"L_stack{m}_fn_{prec}", "stack", (64, 0, m), FN_DEFAULTS, p, u, cc, it, s, prec, 8,
+                       cycles=prec == "fp32")
+            print(f"L_stack{m}_fn_{prec} {p.shape}: iters={it} {s:.2f}s", flush=True)
 
 
 if __name__ == "__main__":

@@ -30,7 +30,7 @@ def test_library_exports_every_header_symbol():
     for s in header_symbols():
         assert hasattr(lib, s), s
         assert s in _lib.SIGNATURES, s
-    assert lib.unw_abi_version() == 1
+    assert lib.unw_abi_version() == 2
 
 
 def test_workspace_bytes_monotone_and_sane():

@@ -268,12 +268,12 @@ def test_solve_4096_fault_matches_reference_cycle_map():
     assert match >= 0.9999, match
 
 
-# RMS bars (rad, after mean removal) against the reference's FP64 run.  The 1e-3 target
-# holds on the G1 grids.  On the 4096^2 fault grid (30 IRLS iterations) float32 rounding alone
-# puts a solver about 1e-3 from the FP64 run: the reference's own float32 path is at 1.0e-3,
-# this solver at 1.2e-3 (and 3e-4 from the reference's float32 run); the cycle maps are
-# identical.  That case is held to 1.5e-3.
-FP64_RMS_BAR = {"L_g1_2048_fn_fp64": 1e-3, "L_g1_4096_fn_fp64": 1e-3, "L_g2_4096_fn_fp64": 1.5e-3}
+# RMS bars (rad, after mean removal) against the reference's FP64 run: 1e-3 on every grid.
+# On the 4096^2 fault grid (30 IRLS iterations) the reference's own float32 path is 1.0e-3
+# from its FP64 run; the error comes from storing the IRLS iterate in float32 (the rounding of
+# u perturbs the residual gradients that set the IRLS weights).  This solver keeps the iterate
+# as a float32 pair (about 48 bits) and lands well inside the bar.
+FP64_RMS_BAR = {"L_g1_2048_fn_fp64": 1e-3, "L_g1_4096_fn_fp64": 1e-3, "L_g2_4096_fn_fp64": 1e-3}
 
 
 @pytest.mark.parametrize("name", sorted(FP64_RMS_BAR))
@@ -297,6 +297,33 @@ def test_full_size_against_reference_fp64(name):
     assert np.sqrt(np.mean((e - e.mean()) ** 2)) <= FP64_RMS_BAR[name]
     assert np.array_equal(np.bincount(cc.ravel().astype(np.int64), minlength=len(d["cc_hist"]))[:len(d["cc_hist"])],
                           d["cc_hist"])
+
+
+def test_stack_members_match_reference():
+    """Members 0-2 of the 64-grid uneven stack (2436x5911, 1838x4122, 1692x6440; Bluestein
+    lengths on both axes; noise sigma 0.36, 0.21, 0.75), solved together in one batched call,
+    against the reference function's own FP32 run (full 2-pi cycle map) and FP64 run (phase on
+    every 8th row and column): cycle map >= 99.99%, RMS <= 1e-3 rad against both runs,
+    identical component sizes."""
+    from core_b200.synthetic import gen_stack_grid, gen_stack_meta
+    names = [f"L_stack{m}_fn_fp32" for m in (0, 1, 2)]
+    if not all(os.path.exists(os.path.join(os.path.dirname(__file__), "golden", n + ".npz")) for n in names):
+        pytest.skip("stack fixtures not generated")
+    meta = gen_stack_meta(64, seed=0)
+    grids = [gen_stack_grid(meta[m]) for m in (0, 1, 2)]
+    out = core_b200.irls_unwrap_2d_batch([g[0] for g in grids], [g[1] for g in grids])
+    for m, (p, c, _), (u, cc) in zip((0, 1, 2), grids, out):
+        d32, d64 = load_golden(f"L_stack{m}_fn_fp32"), load_golden(f"L_stack{m}_fn_fp64")
+        v = np.isfinite(p)
+        assert (np.isnan(u) == ~v).all()
+        assert (cycle_map(u, p) == d32["cycles"])[v].mean() >= 0.9999, m
+        s = int(d32["step"])
+        vs = v[::s, ::s]
+        for d in (d32, d64):
+            e = (u[::s, ::s].astype(np.float64) - d["u_sub"])[vs]
+            assert np.sqrt(np.mean((e - e.mean()) ** 2)) <= 1e-3, (m, str(d["precision"]))
+        h = d32["cc_hist"]
+        assert np.array_equal(np.bincount(cc.ravel().astype(np.int64), minlength=len(h))[:len(h)], h), m
 
 
 def test_batch_equals_single_solves():
