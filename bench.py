@@ -282,8 +282,8 @@ def run_b200(args):
     ws = torch.empty(lib.unw_workspace_bytes(H, W), dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    def solve(flags=0):
-        prm = make_params(**FN)
+    def solve(flags=0, **over):
+        prm = make_params(**dict(FN, **over))
         prm.flags |= flags
         st = _lib.UnwStats()
         rc = lib.unw_solve_f32(ph.data_ptr(), W, wt.data_ptr(), W, H, W, C.byref(prm), out_u.data_ptr(), W,
@@ -312,6 +312,29 @@ def run_b200(args):
     t_dev = ev0.elapsed_time(ev1) / 1e3
     t_dev = barrier_max(t_dev, world, local)
     value = world * npx * args.steps / 1e6 / t_dev
+
+    # ---- the mixed-precision form on the same grid (BASELINE's "mixed vs plain" metric), and
+    # the plain form without CUDA graphs (every launch issued from the host, as the
+    # reference's eager loop does); same K steps, CUDA events
+    def timed(flags, k):
+        for _ in range(2):
+            solve(flags)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(k):
+            st_ = solve(flags)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / 1e3 / k, st_
+    k_alt = max(1, min(args.steps, 5))
+    t_mixed, st_mixed = timed(_lib.UNW_F_MIXED, k_alt)
+    t_nograph, _ = timed(_lib.UNW_F_NO_GRAPH, k_alt)
+    mixed = {"value": round(npx / 1e6 / t_mixed, 3), "unit": UNIT, "ms_per_step": round(t_mixed * 1e3, 3),
+             "col_path": int(st_mixed.col_path), "resid_rel": float(f"{st_mixed.resid_rel:.3g}"),
+             "ratio_mixed_over_plain": round(t_dev / args.steps / t_mixed, 4),
+             "plain_no_graph": {"value": round(npx / 1e6 / t_nograph, 3), "ms_per_step": round(t_nograph * 1e3, 3)},
+             "note": "H = 4096 > 1024: the mixed form keeps the float32 FFT column pass (the tensor-core "
+                     "pass covers grids of at most 1024 rows); see mixed_1024 for where it applies"}
 
     # ---- per-kernel CUDA-event times (UNW_F_PROFILE brackets every launch with an event
     # pair on the solve stream; the events add about 10 us per launch, so this timed pass
@@ -352,6 +375,17 @@ def run_b200(args):
     # ---- accuracy of this run's output against the reference's own runs of the same grid
     # (committed fixtures: full 2-pi cycle map + unwrapped phase on a sub-sampled lattice)
     accuracy = accuracy_vs_reference(p, u_np) if (rank == 0 and args.shape is None) else None
+    if accuracy:
+        # the same grid at the reference run's own IRLS count (tol = 0, max_iter = that count;
+        # cg_tol and the numerical breaks as usual): on this grid rel_change at the 29th
+        # iteration is within about 1% of tol, so the natural stop can differ by one iteration
+        n_ref = reference_irls_count(p, c, None, 1)[0]
+        st_same = solve(0, max_iter=n_ref, tol=0.0)
+        torch.cuda.synchronize()
+        acc_same = accuracy_vs_reference(p, out_u.cpu().numpy())
+        accuracy["natural_stop_irls_iters"] = stats["irls_iters"]
+        accuracy["reference_irls_iters"] = n_ref
+        accuracy["same_irls_iters"] = {"irls_iters": st_same.irls_iters, **(acc_same or {})}
 
     # ---- roofline of the dominant kernel (live event times from the timed region)
     names = _lib.PROF_NAMES
@@ -401,13 +435,21 @@ def run_b200(args):
     # ---- the 64-grid uneven stack (the other workload of the headline metric), sharded by grid
     stack = None
     if not args.no_stack_line:
-        _, sph, swt, s_npx = stack_grids(64, rank, world)
-        s_val, s_t, s_iters = stack_measure(sph, swt, 3, 2, world, local, s_npx)
+        mine, sph, swt, s_npx = stack_grids(64, rank, world)
+        pos = [mine.index(m) for m in (0, 1, 2) if m in mine]
+        s_val, s_t, s_iters, s_out, _ = stack_measure(sph, swt, 3, 2, world, local, s_npx, keep_out=pos)
+        m_val, m_t, _, _, m_paths = stack_measure(sph, swt, 1, 2, world, local, s_npx, flags=_lib.UNW_F_MIXED)
         stack = {"value": round(s_val, 3), "unit": UNIT, "ms_per_step": round(s_t * 1e3, 1), "steps": 2,
                  "warmup": 3, "grids": 64, "total_mpx": round(s_npx / 1e6, 1),
                  "workload": "64 G1 grids, rows U[1500,2600] x cols U[4000,7000], noise U[0.2,0.8], "
                              "function defaults, one batched solve per step, inputs resident in HBM",
-                 "parallelism": f"grids sharded over {world} GPU(s)"}
+                 "parallelism": f"grids sharded over {world} GPU(s)",
+                 "mixed": {"value": round(m_val, 3), "ms_per_step": round(m_t * 1e3, 1),
+                           "ratio_mixed_over_plain": round(m_val / s_val, 4),
+                           "tensor_core_grids": int(sum(m_paths)),
+                           "note": "every stack grid has more than 1024 rows, so the mixed form keeps the "
+                                   "float32 FFT column pass (the tensor-core pass covers H <= 1024)"},
+                 "accuracy": stack_accuracy({mine[k]: s_out[k] for k in s_out}, sph, mine) if rank == 0 else None}
         del sph, swt
 
     # ---- component linking after the unwrap (Stack.unwrap2d's default path)
@@ -438,7 +480,8 @@ def run_b200(args):
                    "path": "core_b200.irls_unwrap_2d(numpy phase, numpy weight) -> numpy (u, conncomp); "
                            "pageable host input, pinned staging for the output"},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches // 1,
-           "stack": stack, "link": link, "accuracy": accuracy}
+           "stack": stack, "link": link, "accuracy": accuracy, "mixed": mixed,
+           "mixed_1024": mixed_small(local) if not args.no_mixed_small else None}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
@@ -470,6 +513,103 @@ def accuracy_vs_reference(p, u):
             "rms_rad": float(f"{np.sqrt(np.mean((e - e.mean()) ** 2)):.3g}"),
             "lattice": f"every {s}th row and column ({int(vs.sum())} valid pixels)"}
     return out or None
+
+
+def stack_accuracy(outs, phases, mine):
+    """Stack members 0-2 against the reference function's FP32 (cycle map) and FP64 runs
+    (tests/golden/L_stack{m}_fn_fp{32,64}.npz)."""
+    res = {}
+    for m, u in sorted(outs.items()):
+        p = phases[mine.index(m)]
+        f32 = os.path.join(REPO, "tests", "golden", f"L_stack{m}_fn_fp32.npz")
+        f64 = os.path.join(REPO, "tests", "golden", f"L_stack{m}_fn_fp64.npz")
+        if not (os.path.exists(f32) and os.path.exists(f64)):
+            continue
+        d32, d64 = np.load(f32), np.load(f64)
+        v = np.isfinite(p)
+        k = np.zeros(p.shape, np.int16)
+        k[v] = np.round((u[v].astype(np.float64) - p[v].astype(np.float64)) / (2 * np.pi)).astype(np.int16)
+        s = int(d32["step"])
+        vs = v[::s, ::s]
+        e = {}
+        for nm, d in (("fp64", d64), ("fp32", d32)):
+            x = (u[::s, ::s].astype(np.float64) - d["u_sub"].astype(np.float64))[vs]
+            e[nm] = float(f"{np.sqrt(np.mean((x - x.mean()) ** 2)):.3g}")
+        res[f"grid{m}"] = {"shape": list(p.shape), "cycle_match_vs_fp32": round(float((k == d32["cycles"])[v].mean()), 6),
+                           "rms_rad_vs_fp64": e["fp64"], "rms_rad_vs_fp32": e["fp32"]}
+    return res or None
+
+
+def mixed_small(local):
+    """The mixed-precision form where it applies (grids of <= 1024 rows): the 1024^2 G1 grid
+    of the reference's fixtures, a batch of 16 such grids (the differentiable-unwrap batch
+    shape) and 64 tiles of 256^2 (a tiled unwrap), plain vs mixed (autotuned) vs mixed with
+    the tensor-core pass forced, device-resident inputs, CUDA events; error of the 1024^2
+    grid against the reference's FP64 run."""
+    import torch
+
+    from core_b200 import _lib
+    from core_b200.irls import make_params
+    from core_b200.synthetic import gen_g1
+    lib = _lib.load()
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    d64 = os.path.join(REPO, "tests", "golden", "L_g1_1024_fn_fp64.npz")
+    for label, count, side in (("g1_1024", 1, 1024), ("batch16_g1_1024", 16, 1024), ("tiles64_g1_256", 64, 256)):
+        grids = [gen_g1(side, side, seed=k) for k in range(count)]
+        n = len(grids)
+        arr = (_lib.UnwGrid * n)()
+        keep = []
+        Hs, Ws = (C.c_int64 * n)(), (C.c_int64 * n)()
+        for k, (p, c, _) in enumerate(grids):
+            ph, wt = torch.from_numpy(p).to(dev), torch.from_numpy(c).to(dev)
+            ou = torch.empty((side, side), dtype=torch.float32, device=dev)
+            oc = torch.empty((side, side), dtype=torch.int16, device=dev)
+            keep += [ph, wt, ou, oc]
+            arr[k] = _lib.UnwGrid(ph.data_ptr(), side, wt.data_ptr(), side, side, side, ou.data_ptr(), side,
+                                  oc.data_ptr(), side)
+            Hs[k] = Ws[k] = side
+        ws = torch.empty(lib.unw_batch_workspace_bytes(n, Hs, Ws), dtype=torch.uint8, device=dev)
+        sts = (_lib.UnwStats * n)()
+        row = {}
+        for mode, flags in (("plain", 0), ("mixed", _lib.UNW_F_MIXED),
+                            ("mixed_tc", _lib.UNW_F_MIXED | _lib.UNW_F_COL_TC)):
+            prm = make_params(**FN)
+            prm.flags |= flags
+
+            def solve():
+                _lib.check(lib.unw_solve_batch(n, arr, C.byref(prm), ws.data_ptr(), ws.numel(), sts,
+                                               stream.cuda_stream))
+            for _ in range(3):
+                solve()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(5):
+                solve()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 1e3 / 5
+            r = {"mpx_s": round(n * side * side / 1e6 / t, 2), "ms_per_step": round(t * 1e3, 3),
+                 "col_path": int(sts[0].col_path), "resid_rel": float(f"{sts[0].resid_rel:.3g}")}
+            if flags & _lib.UNW_F_MIXED:
+                r["tune_ms_fft_tc"] = [round(float(x), 4) for x in sts[0].tune_ms]
+            if side == 1024 and os.path.exists(d64):
+                d = np.load(d64)
+                p = grids[0][0]
+                u = keep[2].cpu().numpy()
+                sl = int(d["step"])
+                vs = np.isfinite(p[::sl, ::sl])
+                x = (u[::sl, ::sl].astype(np.float64) - d["u_sub"])[vs]
+                r["rms_rad_vs_fp64_grid0"] = float(f"{np.sqrt(np.mean((x - x.mean()) ** 2)):.3g}")
+            row[mode] = r
+        row["ratio_mixed_over_plain"] = round(row["mixed"]["mpx_s"] / row["plain"]["mpx_s"], 4)
+        row["ratio_tc_over_plain"] = round(row["mixed_tc"]["mpx_s"] / row["plain"]["mpx_s"], 4)
+        out[label] = row
+        del keep, ws
+        torch.cuda.empty_cache()
+    return out
 
 
 # --------------------------------------------------------------------------- stack workload
@@ -540,9 +680,11 @@ def link_measure(local, steps, warmup):
                         "linksize 5, linkcount 30, IRLS-style labels given"}
 
 
-def stack_measure(phases, weights, warmup, steps, world, local, npx_all):
+def stack_measure(phases, weights, warmup, steps, world, local, npx_all, flags=0, keep_out=()):
     """Batched solves of this rank's grids, inputs resident in HBM: (Mpx/s over the whole
-    stack, seconds per step (max over ranks), per-grid IRLS counts)."""
+    stack, seconds per step (max over ranks), per-grid IRLS counts, {position: u} of the
+    positions in `keep_out` copied to the host, per-grid column paths).  `flags` are extra
+    UNW_F_* bits (e.g. the mixed-precision form)."""
     import torch
 
     from core_b200 import _lib
@@ -567,6 +709,7 @@ def stack_measure(phases, weights, warmup, steps, world, local, npx_all):
     stream = torch.cuda.current_stream(dev)
     sts = (_lib.UnwStats * max(n, 1))()
     prm = make_params(**FN)
+    prm.flags |= flags
 
     def solve():
         if n:
@@ -586,9 +729,11 @@ def stack_measure(phases, weights, warmup, steps, world, local, npx_all):
     barrier(world)
     t = barrier_max(ev0.elapsed_time(ev1) / 1e3, world, local)
     iters = [sts[k].irls_iters for k in range(n)]
+    paths = [sts[k].col_path for k in range(n)]
+    outs = {k: keep[4 * k + 2].cpu().numpy() for k in keep_out if k < n}
     del keep, ws
     torch.cuda.empty_cache()
-    return npx_all * steps / 1e6 / t, t / steps, iters
+    return npx_all * steps / 1e6 / t, t / steps, iters, outs, paths
 
 
 def run_stack(args):
@@ -600,7 +745,7 @@ def run_stack(args):
     mine, phases, weights, npx_all = stack_grids(args.stack, rank, world)
     clocks = ClockSampler(local)
     clocks.start()
-    value, t_step, iters = stack_measure(phases, weights, args.warmup, args.steps, world, local, npx_all)
+    value, t_step, iters, _, _ = stack_measure(phases, weights, args.warmup, args.steps, world, local, npx_all)
     clk = clocks.stop()
     out = {"metric": "unwrapped Mpx/s (64-interferogram uneven stack, function-default iterations)",
            "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -634,6 +779,8 @@ def main():
                     help="leave the 64-grid stack sub-measurement out of the default line")
     ap.add_argument("--no-link-line", action="store_true",
                     help="leave the component-linking sub-measurement out of the default line")
+    ap.add_argument("--no-mixed-small", action="store_true",
+                    help="leave the 1024^2 mixed-precision sub-measurement out of the default line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -11,6 +11,7 @@
 #include <array>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -25,6 +26,7 @@
 namespace {
 
 thread_local char g_err[512];
+thread_local cudaStream_t g_worker_stream = nullptr;  // a launch-group worker thread's own stream
 
 int set_err(int code, const char* fmt, ...) {
     va_list ap;
@@ -154,6 +156,7 @@ struct GridLayout {
 
 struct BatchLayout {
     size_t rowany, colany, bbox, gdev, starts;
+    size_t tcmaps;           // two 128-byte tensor maps per grid (tensor-core column pass)
     std::vector<size_t> base;
     std::vector<GridLayout> g;
     size_t total;
@@ -220,6 +223,7 @@ BatchLayout batch_layout(int n, const long long* H, const long long* W) {
     B.bbox = take(sizeof(int) * 4 * (size_t)n);
     B.gdev = take(sizeof(GridDev) * (size_t)n);
     B.starts = take(sizeof(int) * (size_t)(KS_NKIND + 1) * (2 * (size_t)n + 1));
+    B.tcmaps = take(256 * (size_t)n);
     for (int g = 0; g < n; g++) {
         GridLayout L = grid_layout(H[g], W[g]);
         B.base.push_back(o);
@@ -305,6 +309,7 @@ struct Solver {
     int* dstarts = nullptr;
     Shape sh;
     TcMaps maps;                 // tensor maps of the split DCT matrices (col_tc)
+    void* bmaps = nullptr;       // device: per-grid tensor maps of the pass's float32 sources
     TuneResult tune;             // autotuner timings of the column pass (mixed precision)
     UnwScalars sc{};
     const int* ds(int kind) const { return dstarts + (size_t)kind * (n + 1); }
@@ -341,7 +346,7 @@ cudaError_t L_rowi(Solver& S, int mode) {
                               S.ds(KS_ROWPAIR), S.n);
 }
 cudaError_t L_col(Solver& S, int mode) {
-    if (S.sh.col_tc) return unw_launch_col_tc(mode, S.total[KS_TC], S.s, S.dg, S.ds(KS_TC), S.n, &S.maps);
+    if (S.sh.col_tc) return unw_launch_col_tc(mode, S.total[KS_TC], S.s, S.dg, S.ds(KS_TC), S.n, &S.maps, S.bmaps);
     if (S.sh.col_p2) return unw_launch_col_p2(S.sh.col_p2, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n);
     if (S.sh.col_bl) return unw_launch_col_bl(S.sh.col_bl, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n);
     return unw_launch_col(mode, S.sh.col_T, S.sh.col_emax, S.total[KS_COL], S.sh.col_smem, S.s, S.dg, S.ds(KS_COL),
@@ -396,7 +401,10 @@ cudaStream_t capture_stream() {
 // Returns UNW_OK with both graphs built, or an error code; a failed capture
 // leaves no graph and no stream in capture mode.
 int build_iteration_graphs(Solver& S, IterGraphs& G) {
-    cudaStream_t cs = capture_stream();
+    // a launch-group worker captures on its own stream; otherwise capture runs on this
+    // thread's private stream (the caller's stream may be the legacy default stream,
+    // which cannot be captured, or be shared with other work)
+    cudaStream_t cs = (S.s && S.s == g_worker_stream) ? S.s : capture_stream();
     if (!cs) return set_err(UNW_E_CUDA, "no capture stream");
     cudaStream_t user = S.s;
     for (int par = 0; par < 2; par++) {
@@ -688,7 +696,18 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
     }
     if (tc_h > 0) {
         char* tab = base + B.base[idx[0]] + B.g[idx[0]].tc;
-        const cudaError_t te = B.g[idx[0]].tc ? unw_tc_prepare(tc_h, tab, &S.maps, s) : cudaErrorInvalidValue;
+        cudaError_t te = B.g[idx[0]].tc ? unw_tc_prepare(tc_h, tab, &S.maps, s) : cudaErrorInvalidValue;
+        if (te == cudaSuccess) {
+            // per-grid tensor maps of T and p1 (the pass's float32 sources), 64-byte aligned
+            std::vector<unsigned char> hm(256 * (size_t)n + 64);
+            unsigned char* h = (unsigned char*)up((size_t)hm.data(), 64);
+            for (int g = 0; g < n && te == cudaSuccess; g++) {
+                const GridDev& G = S.hg[g];
+                if (G.H > 0 && !unw_tc_data_maps(G.T, G.p1, G.H, G.W, G.P, h + 256 * (size_t)g)) te = cudaErrorNotSupported;
+            }
+            S.bmaps = base + B.tcmaps + 256 * (size_t)slot;
+            if (te == cudaSuccess) te = cudaMemcpyAsync(S.bmaps, h, 256 * (size_t)n, cudaMemcpyHostToDevice, s);
+        }
         if (te == cudaSuccess) {
             if (prm->flags & UNW_F_COL_TC) {
                 S.sh.col_tc = 1;
@@ -882,20 +901,68 @@ int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, s
     CK(cudaMemcpyAsync(bbox.data(), dbbox, sizeof(int) * 4 * n, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
 
-    // 2. launch groups (kernel configuration per axis), solved one after another
+    // 2. launch groups (kernel configuration per axis).  Several groups run at the same
+    // time, each from its own host thread on its own non-blocking stream, so the GPU
+    // overlaps their kernels and one group's convergence reads do not stall the others;
+    // every input is ready (the bounding-box read above synchronised the caller's
+    // stream) and every output is complete when the call returns (each group ends
+    // with a synchronising state read).  Under UNW_F_PROFILE the groups run one after
+    // another on the caller's stream, so that the per-launch timings stay serial.
     std::map<std::array<int, 4>, std::vector<int>> groups;
     for (int g = 0; g < n; g++)
         groups[group_key(bbox[4 * g + 1] - bbox[4 * g], bbox[4 * g + 3] - bbox[4 * g + 2])].push_back(g);
     if (stats)
         for (int g = 0; g < n; g++) memset(&stats[g], 0, sizeof(unw_stats));
-    int ret = UNW_OK, slot = 0, soff = 0;
-    for (auto& kv : groups) {
-        rc = solve_group(kv.second, grids, bbox, prm, base, B, stats, s, slot, soff);
-        if (rc < 0) return rc;
-        if (rc == UNW_W_NUMERIC) ret = rc;
-        slot += (int)kv.second.size();
-        soff += (KS_NKIND + 1) * ((int)kv.second.size() + 1);
+    struct Job {
+        const std::vector<int>* idx;
+        int slot, soff, rc = UNW_OK;
+        std::string err;
+    };
+    std::vector<Job> jobs;
+    {
+        int slot = 0, soff = 0;
+        for (auto& kv : groups) {
+            Job j;
+            j.idx = &kv.second;
+            j.slot = slot;
+            j.soff = soff;
+            jobs.push_back(j);
+            slot += (int)kv.second.size();
+            soff += (KS_NKIND + 1) * ((int)kv.second.size() + 1);
+        }
     }
+    const bool concurrent = jobs.size() > 1 && !(prm->flags & UNW_F_PROFILE);
+    if (!concurrent) {
+        for (Job& j : jobs) {
+            j.rc = solve_group(*j.idx, grids, bbox, prm, base, B, stats, s, j.slot, j.soff);
+            if (j.rc < 0) return j.rc;
+        }
+    } else {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        std::vector<std::thread> th;
+        for (Job& j : jobs) {
+            th.emplace_back([&, dev, jp = &j] {
+                cudaStream_t gs = nullptr;
+                if (cudaSetDevice(dev) != cudaSuccess ||
+                    cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking) != cudaSuccess) {
+                    jp->rc = set_err(UNW_E_CUDA, "no stream for a launch group");
+                } else {
+                    g_worker_stream = gs;
+                    jp->rc = solve_group(*jp->idx, grids, bbox, prm, base, B, stats, gs, jp->slot, jp->soff);
+                    cudaStreamSynchronize(gs);
+                    cudaStreamDestroy(gs);
+                }
+                if (jp->rc < 0) jp->err = g_err;
+            });
+        }
+        for (auto& t : th) t.join();
+        for (Job& j : jobs)
+            if (j.rc < 0) return set_err(j.rc, "%s", j.err.c_str());
+    }
+    int ret = UNW_OK;
+    for (Job& j : jobs)
+        if (j.rc == UNW_W_NUMERIC) ret = j.rc;
     return ret;
 }
 

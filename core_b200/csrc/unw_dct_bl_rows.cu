@@ -51,8 +51,15 @@ __device__ __forceinline__ float4 upd4(const GridDev& G, float* __restrict__ U, 
     return rn;
 }
 
+// the PCG-start pass (mode 1, once per IRLS iteration) takes half the resident CTAs for
+// the registers of the iterate pair's stencil
+template <int T, int MODE>
+constexpr int bl_rowf_blocks() {
+    return MODE == 1 ? (bl_min_blocks<T>() / 2 > 0 ? bl_min_blocks<T>() / 2 : 1) : bl_min_blocks<T>();
+}
+
 template <class BL, int MODE>
-__global__ void __launch_bounds__(BL::T, bl_min_blocks<BL::T>()) k_rowf_bl(const GridDev* __restrict__ grids,
+__global__ void __launch_bounds__(BL::T, (bl_rowf_blocks<BL::T, MODE>())) k_rowf_bl(const GridDev* __restrict__ grids,
                                                                            const int* __restrict__ starts, int n,
                                                                            int it, int cgk) {
     constexpr int T = BL::T;

@@ -92,8 +92,14 @@ __device__ __forceinline__ float4 rowf_vals4(const GridDev& G, float* __restrict
     }
 }
 
+// The PCG-start pass (mode 1) forms b - A x0 from the iterate pair (eleven float4 rows
+// in flight): it runs once per IRLS iteration and takes half the resident CTAs for the
+// registers that keep it from spilling.
+template <int T, int MODE>
+constexpr int rowf_blocks() { return MODE == 1 ? (min_blocks<T>() / 2 > 0 ? min_blocks<T>() / 2 : 1) : min_blocks<T>(); }
+
 template <int N, int MODE>
-__global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowf_p2(const GridDev* __restrict__ grids,
+__global__ void __launch_bounds__(N / 16, (rowf_blocks<N / 16, MODE>())) k_rowf_p2(const GridDev* __restrict__ grids,
                                                                          const int* __restrict__ starts, int n,
                                                                          int it, int cgk) {
     constexpr int T = N / 16;

@@ -13,13 +13,13 @@
 // A_hi B_hi + A_hi B_lo + A_lo B_hi (three tcgen05.mma kind::f16 issues into one
 // float32 accumulator in tensor memory), about 16 significant bits per term.
 // The DCT matrices are split once per solve into the workspace and staged by
-// TMA (128-byte swizzle); the float32 data are split by the CTA's threads while
-// they are staged into shared memory, so no extra pass over HBM is needed.
+// TMA (128-byte swizzle); the float32 data are staged by TMA too and split by the
+// CTA's threads in shared memory, so no extra pass over HBM is needed.
 //
-// Tiling: one CTA per 128 x 64 output tile, 128 threads; K runs in stages of 64
-// with a two-stage ring (A by TMA, B by the threads), one elected thread issues
-// the MMAs and commits them to the stage's mbarrier; the accumulator (128 lanes
-// x 64 columns of TMEM) is read back with tcgen05.ld by the four warps.  Every
+// Tiling: one CTA per 128 x 64 output tile; K runs in stages of 64 through a
+// three-stage ring (the bf16 A tiles and the float32 B tile by TMA), with one warp
+// loading, one issuing the MMAs and four splitting B into the MMA layout and then
+// reading the accumulator (128 lanes x 64 columns of TMEM) back with tcgen05.ld.  Every
 // wait on an mbarrier is bounded by the global timer: a wait that runs out sets
 // UNW_S_TC_TIMEOUT in the grid's state, the CTA stops issuing, waits (bounded)
 // for the MMAs it committed, frees its tensor memory and returns.
@@ -37,11 +37,13 @@ namespace {
 constexpr int TC_M = 128;                    // output rows per tile (TMEM lanes)
 constexpr int TC_N = 64;                     // output columns per tile (TMEM columns)
 constexpr int TC_K = 64;                     // K per stage: one 128-byte bf16 swizzle row
-constexpr int TC_STAGES = 2;
-constexpr int TC_THREADS = 128;
-constexpr uint32_t TC_A_TILE = TC_M * TC_K * 2;            // 16 KB per split
-constexpr uint32_t TC_B_TILE = TC_K * TC_N * 2;            // 8 KB per split
-constexpr uint32_t TC_STAGE = 2 * TC_A_TILE + 2 * TC_B_TILE;
+constexpr int TC_STAGES = 3;
+constexpr int TC_THREADS = 192;                 // warp 0 loads, warp 1 MMAs, warps 2-5 split / epilogue
+constexpr int TC_CONV_THREADS = 128;
+constexpr uint32_t TC_A_TILE = TC_M * TC_K * 2;            // 16 KB per split (bf16, TMA, swizzled)
+constexpr uint32_t TC_R_TILE = TC_K * TC_N * 4;            // 16 KB float32 B tile (TMA, row-major)
+constexpr uint32_t TC_B_TILE = TC_K * TC_N * 2;            // 8 KB per split (bf16, MMA layout)
+constexpr uint32_t TC_STAGE = 2 * TC_A_TILE + TC_R_TILE + 2 * TC_B_TILE;
 constexpr size_t TC_SMEM = (size_t)TC_STAGES * TC_STAGE + 1024;  // + alignment slack
 constexpr unsigned long long TC_WAIT_NS = 2000000000ull;   // 2 s per wait at most
 constexpr int TC_STATUS_TIMEOUT = 16;                       // UNW_S_TC_TIMEOUT
@@ -57,6 +59,10 @@ __device__ __forceinline__ unsigned long long gtimer() {
 
 __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
@@ -172,15 +178,27 @@ __global__ void k_tc_tables(int H, int Hp, __nv_bfloat16* __restrict__ tab) {
 // ---------------------------------------------------------------- the GEMM
 // EPI 0: first product (X = C T): Y = S .* X -> p1, r.z (MODE >= 1), scalar step
 // EPI 1: second product (T' = E Y): -> T
+//
+// Warp roles (192 threads), no block barrier inside the K loop:
+//   warp 0      one thread issues the TMA loads of each stage (A hi / lo tiles and the
+//               float32 B tile on the stage's `full` mbarrier), TC_STAGES steps ahead,
+//               waiting only for the stage's `empty` mbarrier (its previous MMAs done);
+//   warp 1      one thread waits for the stage's `conv` mbarrier, issues its 12 MMAs and
+//               commits them to `empty`; after the last step it commits to `done`;
+//   warps 2-5   wait for `full`, split the float32 B tile into bf16 hi / lo in the MMA
+//               layout, arrive on `conv`; then the epilogue (warp w reads TMEM lanes
+//               32 (w % 4) .. +31).
 template <int EPI, int MODE>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_col_tc(const GridDev* __restrict__ grids,
                                                           const int* __restrict__ starts, int n,
                                                           const __grid_constant__ CUtensorMap a_hi,
-                                                          const __grid_constant__ CUtensorMap a_lo) {
+                                                          const __grid_constant__ CUtensorMap a_lo,
+                                                          const CUtensorMap* __restrict__ bmaps) {
     extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
-    __shared__ uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES];
+    __shared__ uint64_t full_bar[TC_STAGES], conv_bar[TC_STAGES], empty_bar[TC_STAGES], done_bar;
     __shared__ uint32_t s_tmem;
-    __shared__ int s_fail;
+    __shared__ volatile int s_fail;
+    __shared__ volatile int s_issued;  // K steps whose loads the producer issued
     __shared__ double red[32];
     const int g = find_grid(starts, n, blockIdx.x);
     const GridDev& G = grids[g];
@@ -196,15 +214,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_col_tc(const GridDev* __restr
     const int nk = Hp / TC_K;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     unsigned char* smem = (unsigned char*)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
-    const float* __restrict__ src = EPI == 0 ? G.T : G.p1;
+    // the float32 source of B: T (first product) or Y in p1 (second), one map per grid
+    const CUtensorMap* bmap = bmaps + 2 * g + EPI;
 
     if (tid == 0) {
         for (int s = 0; s < TC_STAGES; s++) {
             mbar_init(&full_bar[s], 1);
+            mbar_init(&conv_bar[s], TC_CONV_THREADS);
             mbar_init(&empty_bar[s], 1);
         }
+        mbar_init(&done_bar, 1);
         s_fail = 0;
+        s_issued = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"((unsigned long long)bmap)
+                     : "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -215,69 +239,37 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_col_tc(const GridDev* __restr
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
+    int committed = -1;  // (warp 1) K steps whose MMAs were committed
 
-    // A tiles of the first stages
-    if (tid == 0) {
-        for (int s = 0; s < TC_STAGES && s < nk; s++) {
-            unsigned char* sa = smem + s * TC_STAGE;
-            mbar_expect_tx(&full_bar[s], 2 * TC_A_TILE);
-            tma_load_2d(sa, &a_hi, &full_bar[s], s * TC_K, m0);
-            tma_load_2d(sa + TC_A_TILE, &a_lo, &full_bar[s], s * TC_K, m0);
-        }
-    }
-    constexpr uint32_t idesc = tc_idesc();
-    int committed = 0;  // MMA groups committed (one per stage use)
-    for (int ks = 0; ks < nk; ks++) {
-        const int s = ks % TC_STAGES;
-        const uint32_t par = (uint32_t)((ks / TC_STAGES) & 1);
-        unsigned char* sa = smem + s * TC_STAGE;
-        unsigned char* sb = sa + 2 * TC_A_TILE;
-        // B: rows k0..k0+63 of the source (K index), columns n0..n0+63, split into bf16
-        // hi / lo, MN-major with the 128-byte swizzle: (k, 16-byte chunk c8) at
-        // (k / 8) * 1024 + (k % 8) * 128 + ((c8 ^ (k % 8)) * 16)
-        const int k0 = ks * TC_K;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int c = tid + q * TC_THREADS;
-            const int kk = c >> 3, c8 = c & 7;
-            const int i = k0 + kk, j = n0 + c8 * 8;
-            float v[8];
-#pragma unroll
-            for (int e = 0; e < 8; e++) v[e] = 0.f;
-            if (i < H) {
-                const float* row = src + (size_t)i * P;
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const int jj = j + 4 * h;
-                    if (jj < W) {  // P >= W and P % 4 == 0: the float4 stays inside the row
-                        const float4 x = *reinterpret_cast<const float4*>(row + jj);
-                        v[4 * h + 0] = x.x;
-                        v[4 * h + 1] = jj + 1 < W ? x.y : 0.f;
-                        v[4 * h + 2] = jj + 2 < W ? x.z : 0.f;
-                        v[4 * h + 3] = jj + 3 < W ? x.w : 0.f;
-                    }
+    if (warp == 0) {
+        if (lane == 0) {
+            for (int ks = 0; ks < nk && !s_fail; ks++) {
+                const int s = ks % TC_STAGES;
+                if (ks >= TC_STAGES && !mbar_wait(&empty_bar[s], (uint32_t)((ks / TC_STAGES - 1) & 1))) {
+                    s_fail = 1;
+                    break;
                 }
+                unsigned char* sa = smem + s * TC_STAGE;
+                mbar_expect_tx(&full_bar[s], 2 * TC_A_TILE + TC_R_TILE);
+                tma_load_2d(sa, &a_hi, &full_bar[s], ks * TC_K, m0);
+                tma_load_2d(sa + TC_A_TILE, &a_lo, &full_bar[s], ks * TC_K, m0);
+                tma_load_2d(sa + 2 * TC_A_TILE, bmap, &full_bar[s], n0, ks * TC_K);  // rows ks*64.., cols n0..
+                s_issued = ks + 1;
             }
-            uint4 hi, lo;
-            float r[8];
-#pragma unroll
-            for (int e = 0; e < 8; e++) r[e] = v[e] - __bfloat162float(__float2bfloat16_rn(v[e]));
-            hi.x = pack_bf16(v[0], v[1]); hi.y = pack_bf16(v[2], v[3]);
-            hi.z = pack_bf16(v[4], v[5]); hi.w = pack_bf16(v[6], v[7]);
-            lo.x = pack_bf16(r[0], r[1]); lo.y = pack_bf16(r[2], r[3]);
-            lo.z = pack_bf16(r[4], r[5]); lo.w = pack_bf16(r[6], r[7]);
-            const uint32_t off = (uint32_t)((kk >> 3) * 1024 + (kk & 7) * 128 + ((c8 ^ (kk & 7)) << 4));
-            *reinterpret_cast<uint4*>(sb + off) = hi;
-            *reinterpret_cast<uint4*>(sb + TC_B_TILE + off) = lo;
         }
-        fence_proxy_async();
-        __syncthreads();
-        if (tid == 0 && !s_fail) {
-            if (!mbar_wait(&full_bar[s], par)) {
-                s_fail = 1;
-            } else {
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = tc_idesc();
+            committed = 0;
+            for (int ks = 0; ks < nk && !s_fail; ks++) {
+                const int s = ks % TC_STAGES;
+                if (!mbar_wait(&conv_bar[s], (uint32_t)((ks / TC_STAGES) & 1))) {
+                    s_fail = 1;
+                    break;
+                }
                 tc_fence_after();
-                const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
+                unsigned char* sa = smem + s * TC_STAGE;
+                const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sa + 2 * TC_A_TILE + TC_R_TILE);
 #pragma unroll
                 for (int kk = 0; kk < TC_K / 16; kk++) {
                     // A: +32 bytes per 16 K inside the swizzle row; B: +2 swizzle atoms (16 rows)
@@ -292,32 +284,69 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_col_tc(const GridDev* __restr
                 }
                 umma_commit(&empty_bar[s]);
                 committed = ks + 1;
-                // this stage's MMAs must finish before its buffers are refilled
-                if (!mbar_wait(&empty_bar[s], par)) {
-                    s_fail = 1;
-                } else if (ks + TC_STAGES < nk) {
-                    mbar_expect_tx(&full_bar[s], 2 * TC_A_TILE);
-                    tma_load_2d(sa, &a_hi, &full_bar[s], (ks + TC_STAGES) * TC_K, m0);
-                    tma_load_2d(sa + TC_A_TILE, &a_lo, &full_bar[s], (ks + TC_STAGES) * TC_K, m0);
-                }
             }
+            umma_commit(&done_bar);  // completes once every MMA issued above has finished
         }
-        __syncthreads();  // the stage's B buffers are free again / s_fail is visible
-        if (s_fail) break;
+    } else {
+        // split B: row kk, 16-byte chunk c8 (8 columns) -> MN-major, 128-byte swizzle:
+        // (kk / 8) * 1024 + (kk % 8) * 128 + ((c8 ^ (kk % 8)) * 16)
+        const int ct = tid - 64;
+        for (int ks = 0; ks < nk; ks++) {
+            const int s = ks % TC_STAGES;
+            if (s_fail || !mbar_wait(&full_bar[s], (uint32_t)((ks / TC_STAGES) & 1))) {
+                s_fail = 1;
+                break;
+            }
+            unsigned char* sa = smem + s * TC_STAGE;
+            const unsigned char* sr = sa + 2 * TC_A_TILE;
+            unsigned char* sb = sa + 2 * TC_A_TILE + TC_R_TILE;
+#pragma unroll
+            for (int q = 0; q < (TC_K * TC_N / 8) / TC_CONV_THREADS; q++) {
+                const int c = ct + q * TC_CONV_THREADS;
+                const int kk = c >> 3, c8 = c & 7;
+                const float4 x0 = *reinterpret_cast<const float4*>(sr + kk * 256 + c8 * 32);
+                const float4 x1 = *reinterpret_cast<const float4*>(sr + kk * 256 + c8 * 32 + 16);
+                const float v[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+                float r[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) r[e] = v[e] - __bfloat162float(__float2bfloat16_rn(v[e]));
+                uint4 hi, lo;
+                hi.x = pack_bf16(v[0], v[1]); hi.y = pack_bf16(v[2], v[3]);
+                hi.z = pack_bf16(v[4], v[5]); hi.w = pack_bf16(v[6], v[7]);
+                lo.x = pack_bf16(r[0], r[1]); lo.y = pack_bf16(r[2], r[3]);
+                lo.z = pack_bf16(r[4], r[5]); lo.w = pack_bf16(r[6], r[7]);
+                const uint32_t off = (uint32_t)((kk >> 3) * 1024 + (kk & 7) * 128 + ((c8 ^ (kk & 7)) << 4));
+                *reinterpret_cast<uint4*>(sb + off) = hi;
+                *reinterpret_cast<uint4*>(sb + TC_B_TILE + off) = lo;
+            }
+            fence_proxy_async();
+            mbar_arrive(&conv_bar[s]);
+        }
     }
-    // every committed MMA group has been waited for (thread 0 waits right after each
-    // commit); outstanding A loads of a failed run are waited for here, bounded
-    if (tid == 0 && s_fail) {
-        for (int ks = committed; ks < nk && ks < committed + TC_STAGES; ks++)
-            mbar_wait(&full_bar[ks % TC_STAGES], (uint32_t)((ks / TC_STAGES) & 1));
-        atomicOr(&st->status, TC_STATUS_TIMEOUT);
+    // every MMA issued has finished once `done` completes (bounded); a failed run also
+    // waits (bounded) for the loads it issued, so nothing is in flight when TMEM is freed
+    if (warp == 1 && lane == 0 && committed >= 0) {
+        if (!mbar_wait(&done_bar, 0)) s_fail = 1;
+    }
+    __syncthreads();
+    if (s_fail) {
+        if (tid == 0) {
+            // the last load issued into each stage completes that stage's phase
+            // (ks / TC_STAGES) & 1; earlier phases of the stage have completed already
+            const int issued = s_issued;
+            for (int ks = issued - TC_STAGES < 0 ? 0 : issued - TC_STAGES; ks < issued; ks++)
+                mbar_wait(&full_bar[ks % TC_STAGES], (uint32_t)((ks / TC_STAGES) & 1));
+            atomicOr(&st->status, TC_STATUS_TIMEOUT);
+        }
+        __syncthreads();
     }
     tc_fence_after();
     double acc[1] = {0.0};
-    if (!s_fail) {
-        // epilogue: thread = TMEM lane = output row m0 + 32 warp + lane
-        const int row = m0 + warp * 32 + lane;
-        const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
+    if (!s_fail && warp >= 2) {
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 = output rows m0 + that range
+        const int quarter = warp & 3;
+        const int row = m0 + quarter * 32 + lane;
+        const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16);
         if (EPI == 0) {
             const float negs = -1.0f / (4.0f * (float)H * (float)W);
             const float ck = row < H ? __ldg(&G.sH[row]) : 1.f;
@@ -410,13 +439,27 @@ bool make_map(CUtensorMap* m, const void* plane, int Hp) {
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// float32 H x W array with a row pitch of P floats, box 64 (columns) x 64 (rows), no
+// swizzle; reads beyond the array are zero-filled
+bool make_data_map(CUtensorMap* m, const float* base, int H, int W, int P) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)W, (cuuint64_t)H};
+    cuuint64_t strides[1] = {(cuuint64_t)P * 4};
+    cuuint32_t box[2] = {(cuuint32_t)TC_N, (cuuint32_t)TC_K};
+    cuuint32_t estr[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int EPI, int MODE>
 cudaError_t go(int nblk, cudaStream_t s, const GridDev* gd, const int* starts, int n, const CUtensorMap& hi,
-               const CUtensorMap& lo) {
+               const CUtensorMap& lo, const CUtensorMap* bmaps) {
     auto kfn = k_col_tc<EPI, MODE>;
     cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
     if (e != cudaSuccess) return e;
-    kfn<<<nblk, TC_THREADS, TC_SMEM, s>>>(gd, starts, n, hi, lo);
+    kfn<<<nblk, TC_THREADS, TC_SMEM, s>>>(gd, starts, n, hi, lo, bmaps);
     return cudaGetLastError();
 }
 
@@ -447,18 +490,25 @@ cudaError_t unw_tc_prepare(int H, void* tab, TcMaps* maps, cudaStream_t s) {
     return cudaSuccess;
 }
 
+bool unw_tc_data_maps(const float* T, const float* Y, int H, int W, int P, void* out2) {
+    if ((P & 3) || ((uintptr_t)T & 15) || ((uintptr_t)Y & 15)) return false;
+    CUtensorMap* m = (CUtensorMap*)out2;
+    return make_data_map(m, T, H, W, P) && make_data_map(m + 1, Y, H, W, P);
+}
+
 cudaError_t unw_launch_col_tc(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts, int n,
-                              const TcMaps* maps) {
+                              const TcMaps* maps, const void* bmaps) {
     if (nblk <= 0) return cudaSuccess;
     const CUtensorMap& ch = *(const CUtensorMap*)maps->c_hi;
     const CUtensorMap& cl = *(const CUtensorMap*)maps->c_lo;
     const CUtensorMap& eh = *(const CUtensorMap*)maps->e_hi;
     const CUtensorMap& el = *(const CUtensorMap*)maps->e_lo;
+    const CUtensorMap* bm = (const CUtensorMap*)bmaps;
     cudaError_t e;
     switch (mode) {
-        case 0: e = go<0, 0>(nblk, s, gd, starts, n, ch, cl); if (e == cudaSuccess) e = go<1, 0>(nblk, s, gd, starts, n, eh, el); break;
-        case 1: e = go<0, 1>(nblk, s, gd, starts, n, ch, cl); if (e == cudaSuccess) e = go<1, 1>(nblk, s, gd, starts, n, eh, el); break;
-        default: e = go<0, 2>(nblk, s, gd, starts, n, ch, cl); if (e == cudaSuccess) e = go<1, 2>(nblk, s, gd, starts, n, eh, el); break;
+        case 0: e = go<0, 0>(nblk, s, gd, starts, n, ch, cl, bm); if (e == cudaSuccess) e = go<1, 0>(nblk, s, gd, starts, n, eh, el, bm); break;
+        case 1: e = go<0, 1>(nblk, s, gd, starts, n, ch, cl, bm); if (e == cudaSuccess) e = go<1, 1>(nblk, s, gd, starts, n, eh, el, bm); break;
+        default: e = go<0, 2>(nblk, s, gd, starts, n, ch, cl, bm); if (e == cudaSuccess) e = go<1, 2>(nblk, s, gd, starts, n, eh, el, bm); break;
     }
     return e;
 }

@@ -252,7 +252,7 @@ int unw_goldstein_c64(const float* phase, int64_t phase_pitch, const float* corr
         return unw_set_error(UNW_E_CUDA, cudaGetErrorString(e));
     k_gs_weights<<<1, 256, 0, s>>>(const_cast<float*>(a.wgt), psize_y, psize_x);
     const size_t smem = 2 * sizeof(float2) * (size_t)psize_y * psize_x;
-    cudaFuncSetAttribute(k_gs_patch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    unw_smem_limit((const void*)k_gs_patch);
     for (int c = 0; c < 4; c++) {
         const int ci = c >> 1, cj = c & 1;
         const long long np = (long long)((a.npy - ci + 1) / 2) * ((a.npx - cj + 1) / 2);

@@ -1,7 +1,36 @@
 // Host-side declarations of the kernel launchers (implemented in the .cu files).
 #pragma once
 #include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "unw_internal.cuh"
+
+// Raises a kernel's dynamic shared-memory limit to the most one CTA can have on the
+// current device (the opt-in maximum less the kernel's static shared memory), once per
+// kernel and device.  Launches may then pass any dynamic size up to that.  Kernels whose
+// launches use different dynamic sizes use this instead of setting the limit to each
+// launch's size: with launches from several host threads (a batch's launch groups run
+// concurrently) a smaller setting from one thread could land between another thread's
+// setting and its launch, which then fails.
+inline cudaError_t unw_smem_limit(const void* kfn) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({kfn, dev})) return cudaSuccess;
+    cudaFuncAttributes a;
+    int optin = 0;
+    if ((e = cudaFuncGetAttributes(&a, kfn)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes);
+    if (e == cudaSuccess) done[{kfn, dev}] = 1;
+    return e;
+}
 
 struct UnwScalars {
     int max_iter;
@@ -71,8 +100,11 @@ struct TcMaps {                       // four CUtensorMap (128 bytes each): C hi
 size_t unw_tc_table_bytes(int H);     // workspace bytes of the split DCT matrices (0 if H > UNW_TC_MAX_H)
 int unw_tc_ctas(int H, int W);        // CTAs of one grid's tensor-core column pass
 cudaError_t unw_tc_prepare(int H, void* tab, TcMaps* maps, cudaStream_t s);
+// per-grid tensor maps of the pass's float32 sources T and Y (p1), H x W with pitch P:
+// two 128-byte CUtensorMap objects written to out2 (64-byte aligned host memory)
+bool unw_tc_data_maps(const float* T, const float* Y, int H, int W, int P, void* out2);
 cudaError_t unw_launch_col_tc(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts, int n,
-                              const TcMaps* maps);
+                              const TcMaps* maps, const void* bmaps);
 
 // bounding box of valid pixels on the caller's full grid
 cudaError_t unw_launch_bbox(const float* phase, long long pitch, int H0, int W0, int* rowany,

@@ -954,7 +954,7 @@ int unw_link_pairs_f32(const float* phase, int64_t phase_pitch, const uint16_t* 
         int threads = 256;
         while (threads > 32 && (size_t)threads * K * 12 > 96 * 1024) threads >>= 1;
         const size_t smem = (size_t)threads * K * 12;
-        LK_CK(cudaFuncSetAttribute(k_lk_nbr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        LK_CK(unw_smem_limit((const void*)k_lk_nbr));
         const int rows = std::max(1, LK_NBR_CHUNK / K);
         std::vector<int> hn((size_t)rows * K);
         for (int c0 = 0; c0 < n; c0 += rows) {

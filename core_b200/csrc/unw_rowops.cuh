@@ -19,12 +19,13 @@ __device__ __forceinline__ float lap_at(const float* __restrict__ x, const float
     return -res;
 }
 
-// Difference a - b of two iterate values held as float32 pairs.  fl(ah - bh) carries a
-// rounding error relative to the difference itself (not to |u|), and the low parts add
-// back what the storage of u in float32 would lose, so the result equals the exact
-// difference to a few float32 ulps of the difference.
+// Difference a - b of two iterate values held as float32 pairs: exact in float64,
+// rounded once to float32.  (A float32 form, fl(fl(ah - bh) + fl(al - bl)), is within a
+// few ulps of the difference too; on the 4096^2 fault grid, whose IRLS stop test is
+// decided by rel_change within about 1% of tol at the 29th iteration, that form ended
+// after 29 iterations where the reference's FP64 run takes 30, and this one takes 30.)
 __device__ __forceinline__ float pair_diff(float ah, float al, float bh, float bl) {
-    return fadd(fsub(ah, bh), fsub(al, bl));
+    return __double2float_rn(((double)ah - (double)bh) + ((double)al - (double)bl));
 }
 
 // A x at (i, j) for the iterate x = U + L held as a float32 pair: the reference's op

@@ -278,16 +278,25 @@ FP64_RMS_BAR = {"L_g1_2048_fn_fp64": 1e-3, "L_g1_4096_fn_fp64": 1e-3, "L_g2_4096
 
 @pytest.mark.parametrize("name", sorted(FP64_RMS_BAR))
 def test_full_size_against_reference_fp64(name):
-    """Full-size grids against the reference's FP64 run of the same algorithm
-    (function defaults): 2-pi cycle map on >= 99.99% of valid pixels, RMS after
-    mean removal within FP64_RMS_BAR on the stored lattice, identical component sizes."""
+    """Full-size grids against the reference's FP64 run of the same algorithm, with the
+    same IRLS iteration count (function defaults, tol = 0 and max_iter = the reference
+    run's count; cg_tol and every numerical break as usual): 2-pi cycle map on >= 99.99%
+    of valid pixels, RMS after mean removal within FP64_RMS_BAR on the stored lattice,
+    identical component sizes.  The natural stop (tol = 1e-3) must land within one
+    iteration of the reference's: on the fault grid rel_change at the 29th iteration is
+    within about 1% of tol in every float32 and mixed variant measured, so which side of
+    tol it falls on is decided by rounding."""
     path = os.path.join(os.path.dirname(__file__), "golden", name + ".npz")
     if not os.path.exists(path):
         pytest.skip(name + " not generated")
     d = load_golden(name)
     H, W, seed = [int(x) for x in d["gen_args"]]
     p, c, _ = gen_g1(H, W, seed=seed) if str(d["gen"]) == "g1" else gen_g2(H, W, seed=seed)
-    u, cc = core_b200.irls_unwrap_2d(p, c, **d["kw"])
+    n_ref = int(d["iters"])
+    _, _, st = core_b200.irls_unwrap_2d(p, c, return_stats=True, **d["kw"])
+    assert abs(st["irls_iters"] - n_ref) <= 1, (st["irls_iters"], n_ref)
+    u, cc, st = core_b200.irls_unwrap_2d(p, c, return_stats=True, **dict(d["kw"], max_iter=n_ref, tol=0.0))
+    assert st["irls_iters"] == n_ref
     v = np.isfinite(p)
     assert (np.isnan(u) == ~v).all()
     assert (cycle_map(u, p) == d["cycles"])[v].mean() >= 0.9999
