@@ -40,6 +40,14 @@ sys.path.insert(0, REPO)
 
 FN = dict(max_iter=50, tol=1e-3, cg_max_iter=20, cg_tol=1e-4, epsilon=1e-2, conncomp_size=30)
 METRIC = "unwrapped Mpx/s (4096^2 fault grid, function-default iterations)"
+
+
+def metric_name(shape_arg):
+    """The metric label of the workload run: the 4096^2 fault grid by default, else the
+    --shape grid of the smooth generator."""
+    if shape_arg is None:
+        return METRIC
+    return f"unwrapped Mpx/s ({int(shape_arg[0])}x{int(shape_arg[1])} smooth grid, function-default iterations)"
 UNIT = "Mpx/s"
 
 # Algorithmic HBM bytes per pixel per launch of each kernel family (float32 words,
@@ -240,7 +248,7 @@ def run_reference(args):
            "cpu_model": cpu_model(), "os_cpu_count": os.cpu_count(), "scipy_fft_workers": workers,
            "numpy_threads_note": "the oracle's FFTs run on scipy.fft with workers=cores; its elementwise "
                                  "numpy work is single-threaded"}
-    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+    out = {"metric": metric_name(args.shape), "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": t_irls * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
            "config": workload_config(p.shape, args.shape, args.gpus),
@@ -265,7 +273,7 @@ def run_b200(args):
 
     import core_b200
     from core_b200 import _lib
-    from core_b200.irls import make_params
+    from core_b200.irls import make_params, precision_flags
 
     rank, world, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
@@ -282,9 +290,11 @@ def run_b200(args):
     ws = torch.empty(lib.unw_workspace_bytes(H, W), dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
+    base_flags = precision_flags(args.precision, args.col_pass)
+
     def solve(flags=0, **over):
         prm = make_params(**dict(FN, **over))
-        prm.flags |= flags
+        prm.flags |= flags | base_flags
         st = _lib.UnwStats()
         rc = lib.unw_solve_f32(ph.data_ptr(), W, wt.data_ptr(), W, H, W, C.byref(prm), out_u.data_ptr(), W,
                                out_cc.data_ptr(), W, ws.data_ptr(), ws.numel(), C.byref(st), stream.cuda_stream)
@@ -333,8 +343,9 @@ def run_b200(args):
              "col_path": int(st_mixed.col_path), "resid_rel": float(f"{st_mixed.resid_rel:.3g}"),
              "ratio_mixed_over_plain": round(t_dev / args.steps / t_mixed, 4),
              "plain_no_graph": {"value": round(npx / 1e6 / t_nograph, 3), "ms_per_step": round(t_nograph * 1e3, 3)},
-             "note": "H = 4096 > 1024: the mixed form keeps the float32 FFT column pass (the tensor-core "
-                     "pass covers grids of at most 1024 rows); see mixed_1024 for where it applies"}
+             "note": (f"H = {H} > 1024: the mixed form keeps the float32 FFT column pass (the tensor-core "
+                      "pass covers grids of at most 1024 rows); see mixed_1024 for where it applies")
+             if H > 1024 else "H <= 1024: the autotuner chose col_path (0 FFT, 1 tensor cores)"}
 
     # ---- per-kernel CUDA-event times (UNW_F_PROFILE brackets every launch with an event
     # pair on the solve stream; the events add about 10 us per launch, so this timed pass
@@ -356,15 +367,16 @@ def run_b200(args):
     # input copied to the device and numpy output copied back inside the timed region
     # warm-up in the timed loop's own pattern: a caller that keeps the previous
     # result while the next call runs holds two pinned output blocks
+    pkw = dict(precision=args.precision, col_pass=args.col_pass)
     for _ in range(2):
-        u_np, cc_np = core_b200.irls_unwrap_2d(p, c, device=dev, **FN)
+        u_np, cc_np = core_b200.irls_unwrap_2d(p, c, device=dev, **FN, **pkw)
     torch.cuda.synchronize()
     barrier(world)
     e2e_steps = max(1, min(args.steps, 3))
     t = time.perf_counter()
     ev0.record(stream)
     for _ in range(e2e_steps):
-        u_np, cc_np = core_b200.irls_unwrap_2d(p, c, device=dev, **FN)
+        u_np, cc_np = core_b200.irls_unwrap_2d(p, c, device=dev, **FN, **pkw)
     ev1.record(stream)
     torch.cuda.synchronize()
     t_e2e = max(ev0.elapsed_time(ev1) / 1e3, time.perf_counter() - t)
@@ -468,11 +480,13 @@ def run_b200(args):
                           f"extrapolated to {stats['irls_iters']} IRLS iterations = {full:.0f}s")}
 
     launches = int(prof_n.sum()) // prof_steps * args.steps  # same deterministic launch sequence per step
-    out = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    out = {"metric": metric_name(args.shape), "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+           "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(t_dev / args.steps * 1e3, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
            "config": dict(workload_config((H, W), args.shape, world),
                           step="one full unwrap per step, one replica per GPU",
+                          precision=args.precision, col_pass=args.col_pass,
                           irls_iters=stats["irls_iters"], pcg_iters=stats["cg_iters_total"],
                           l2="inputs 134 MB and solver working set ~1.1 GB exceed the 126 MB L2"),
            "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(npx * 8),
@@ -779,6 +793,10 @@ def main():
                     help="leave the 64-grid stack sub-measurement out of the default line")
     ap.add_argument("--no-link-line", action="store_true",
                     help="leave the component-linking sub-measurement out of the default line")
+    ap.add_argument("--precision", default="plain", choices=["plain", "mixed"],
+                    help="precision form of the main line's solves (default: plain float32)")
+    ap.add_argument("--col-pass", default="auto", choices=["auto", "tc", "fft"],
+                    help="with --precision mixed: column pass chosen by the autotuner, or forced")
     ap.add_argument("--no-mixed-small", action="store_true",
                     help="leave the 1024^2 mixed-precision sub-measurement out of the default line")
     args = ap.parse_args()

@@ -41,6 +41,8 @@ def irls_adjoint(phase, weight, u, grad_u, *, cg_max_iter=1000, cg_tol=1e-6, eps
                                  C.byref(st), torch.cuda.current_stream(dev).cuda_stream)
     _lib.check(rc, "unw_adjoint_f32")
     stats = {"refine_cg_iters": int(st.cg_iters[0]), "adjoint_cg_iters": int(st.cg_iters[1]),
+             "refine_pass_cg_iters": [int(st.cg_iters[2 + k]) for k in range(3)],
+             "refine_rel_residual": float(st.resid_rel),
              "adjoint_rel_residual": float(st.rel_change), "status": int(st.status), "numeric_warning": rc == 1}
     return gph, gw, stats
 

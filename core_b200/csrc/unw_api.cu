@@ -1059,7 +1059,30 @@ int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_
     //    the relative tolerance from u: u* in U1
     rc = enqueue_iteration(S, 0);
     if (rc) return rc;
-    // 2. components of the valid mask and the per-component sin/cos sums at u*
+    // 2. iterative refinement of u* on the frozen system: residual in float64 (phase
+    //    differences in float64), correction by the PCG from x0 = 0, added to the pair; the
+    //    last REFINE only measures the residual of the final u*.  Before the post pipeline,
+    //    which sets u* to NaN outside the valid pixels (its shift is 0 here: no median ran)
+    for (int k = 0; k <= UNW_ADJ_REFINE; k++) {
+        CK(unw_launch_adj(UNW_A_REARM, 1, s, S.dg, nullptr, n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
+        CK(unw_launch_adj(UNW_A_REFINE, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr,
+                          0, 0));
+        if (k == UNW_ADJ_REFINE) break;
+        CK(unw_launch_adj(UNW_A_REFINE, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr,
+                          0, 1));
+        CK(L_rowf(S, 1, 1, 0));
+        CK(L_col(S, 1));
+        CK(L_rowi(S, 1));
+        for (int c = 0; c < S.sc.cg_max_iter; c++) {
+            CK(unw_launch_simple(UNW_K_MATVEC, S.total[KS_MATVEC], s, S.dg, S.ds(KS_MATVEC), n, c, S.sc));
+            CK(L_rowf(S, 2, 1, c));
+            CK(L_col(S, 2));
+            CK(L_rowi(S, 2));
+        }
+        CK(unw_launch_adj(UNW_A_ADDD, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0,
+                          k));
+    }
+    // 3. components of the valid mask
     const int nt = S.total[KS_NKIND];
     CK(unw_launch_post(UNW_P_SHIFT_CCINIT, ne, s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
     CK(unw_launch_post(UNW_P_UNION, ne, s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
@@ -1067,9 +1090,10 @@ int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_
     CK(unw_launch_post(UNW_P_TILESCAN, n, s, S.dg, nullptr, n, S.sc, S.hg.data()));
     CK(unw_launch_post(UNW_P_LABEL, nt, s, S.dg, S.ds(KS_NKIND), n, S.sc, S.hg.data()));
     CK(unw_launch_post(UNW_P_ACCUM, ne, s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
-    // 3. adjoint right-hand side through the alignment, then lambda = A^+ G' (x0 = 0 in U0/L0,
+    // 4. adjoint right-hand side through the alignment, then lambda = A^+ G' (x0 = 0 in U0/L0,
     //    lambda accumulated in D)
     CK(cudaMemsetAsync(S.hg[0].adj, 0, sizeof(double) * (size_t)S.hg[0].lab_cap, s));
+    CK(cudaMemsetAsync(S.hg[0].csum, 0, sizeof(double) * 4 * (size_t)S.hg[0].lab_cap, s));
     CK(unw_launch_adj(UNW_A_LSUM, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
     CK(unw_launch_adj(UNW_A_RHS, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
     CK(unw_launch_adj(UNW_A_REARM, 1, s, S.dg, nullptr, n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
@@ -1082,7 +1106,7 @@ int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_
         CK(L_col(S, 2));
         CK(L_rowi(S, 2));
     }
-    // 4. gradients
+    // 5. gradients
     CK(unw_launch_adj(UNW_A_GRAD, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, gph, gph_pitch, gw,
                       gw_pitch));
     std::vector<InstState> hs;
@@ -1096,6 +1120,11 @@ int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_
         o.cg_iters[1] = st.cg_iter;
         o.cg_iters_last = st.cg_iter;
         o.cg_iters_total = st.cg_log[0] + st.cg_iter;
+        for (int k = 0; k < UNW_ADJ_REFINE; k++) {
+            o.cg_iters[2 + k] = st.cg_log[2 + k];
+            o.cg_iters_total += st.cg_log[2 + k];
+        }
+        o.resid_rel = st.resid_rel;
         o.n_labels = st.n_labels;
         o.status = st.status;
         // relative residual of the adjoint solve (cg_tol = cg_rel * ||r0||)

@@ -60,19 +60,19 @@ __device__ __forceinline__ float4 rowf_vals4(const GridDev& G, float* __restrict
         const float xl = j > 0 ? U[o - 1] : 0.f, ll = j > 0 ? Lo[o - 1] : 0.f;
         const float wxl = j > 0 ? G.wIx[o - 1] : 0.f;
         const float xr = j + 4 < W ? U[o + 4] : 0.f, lr = j + 4 < W ? Lo[o + 4] : 0.f;
-        const float xs[6] = {xl, x4.x, x4.y, x4.z, x4.w, xr};
-        const float ls[6] = {ll, l4.x, l4.y, l4.z, l4.w, lr};
+        const double xs[6] = {pair_val(xl, ll), pair_val(x4.x, l4.x), pair_val(x4.y, l4.y), pair_val(x4.z, l4.z),
+                              pair_val(x4.w, l4.w), pair_val(xr, lr)};
         const float wxs[5] = {wxl, wx4.x, wx4.y, wx4.z, wx4.w};
         float out[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int jj = j + q;
-            const float xc = xs[q + 1], lc = ls[q + 1];
+            const double xc = xs[q + 1];
             float res = 0.f;
-            if (jj > 0) res = fsub(res, fmul(pair_diff(xc, lc, xs[q], ls[q]), wxs[q]));
-            if (jj < W - 1) res = fadd(res, fmul(pair_diff(xs[q + 2], ls[q + 2], xc, lc), wxs[q + 1]));
-            if (i > 0) res = fsub(res, fmul(pair_diff(xc, lc, f4get(xu4, q), f4get(lu4, q)), f4get(wyu4, q)));
-            if (i < H - 1) res = fadd(res, fmul(pair_diff(f4get(xd4, q), f4get(ld4, q), xc, lc), f4get(wy4, q)));
+            if (jj > 0) res = fsub(res, fmul(dpair_diff(xc, xs[q]), wxs[q]));
+            if (jj < W - 1) res = fadd(res, fmul(dpair_diff(xs[q + 2], xc), wxs[q + 1]));
+            if (i > 0) res = fsub(res, fmul(dpair_diff(xc, pair_val(f4get(xu4, q), f4get(lu4, q))), f4get(wyu4, q)));
+            if (i < H - 1) res = fadd(res, fmul(dpair_diff(pair_val(f4get(xd4, q), f4get(ld4, q)), xc), f4get(wy4, q)));
             const float val = fsub(f4get(b4, q), -res);
             out[q] = val;
             acc[0] += isfinite(val) ? 0.0 : 1.0;

@@ -62,6 +62,7 @@ struct InstState {
     double resid_rel;           // ||b - A u|| / ||b|| of the final system in float64 (k_resid)
     float tol, cg_tol, eps2;
     float cg_rel;               // > 0: cg_tol = cg_rel * ||r0|| at the PCG start
+    double refine_scale;        // adjoint refinement: scale of the correction's right-hand side
     int cg_max_iter;
     int cg_total;
     int cg_log[UNW_MAX_LOG];

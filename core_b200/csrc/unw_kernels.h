@@ -129,13 +129,16 @@ cudaError_t unw_launch_post(int which, int nblk, cudaStream_t s, const GridDev* 
                             int n, const UnwScalars& sc, const GridDev* host_grids);
 
 // frozen-weight adjoint (KS_ELEM shapes except REARM)
+#define UNW_ADJ_REFINE 3    // refinement passes of u* (each stops early below 1e-13 residual)
 enum {
     UNW_A_LOAD = 0,     // forward output and dL/dout into the crop
     UNW_A_LSUM,         // per-component sum of dL/dout
     UNW_A_RHS,          // adjoint right-hand side, x0 = 0
     UNW_A_REARM,        // solver state for the adjoint PCG
-    UNW_A_GRAD          // dL/dphase, dL/dweight
+    UNW_A_GRAD,         // dL/dphase, dL/dweight
+    UNW_A_REFINE,       // float64 residual of the frozen system at u* -> correction right-hand side
+    UNW_A_ADDD          // u* += correction (pass k)
 };
 cudaError_t unw_launch_adj(int which, int nblk, cudaStream_t s, const GridDev* gd, const int* starts, int n,
                            const float* a, long long ap, const float* b, long long bp, float* c, long long cp,
-                           float* d, long long dp);
+                           float* d, long long dp, int k = 0);

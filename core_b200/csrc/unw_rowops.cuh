@@ -27,6 +27,10 @@ __device__ __forceinline__ float lap_at(const float* __restrict__ x, const float
 __device__ __forceinline__ float pair_diff(float ah, float al, float bh, float bl) {
     return __double2float_rn(((double)ah - (double)bh) + ((double)al - (double)bl));
 }
+// The same from the pairs' float64 values (hi + lo is exact in float64, and so is each of
+// the two differences above; both forms round the exact difference once): each pixel's
+// pair is converted once and shared by the differences it takes part in.
+__device__ __forceinline__ float dpair_diff(double a, double b) { return __double2float_rn(a - b); }
 
 // A x at (i, j) for the iterate x = U + L held as a float32 pair: the reference's op
 // order (lap_at), each neighbour difference formed from the pair by pair_diff.
@@ -34,12 +38,12 @@ __device__ __forceinline__ float lap_at_pair(const float* __restrict__ U, const 
                                              const float* __restrict__ wx, const float* __restrict__ wy, int i, int j,
                                              int H, int W, int P) {
     const size_t o = (size_t)i * P + j;
-    const float uc = U[o], lc = L[o];
+    const double xc = pair_val(U[o], L[o]);
     float res = 0.f;
-    if (j > 0) res = fsub(res, fmul(pair_diff(uc, lc, U[o - 1], L[o - 1]), wx[o - 1]));
-    if (j < W - 1) res = fadd(res, fmul(pair_diff(U[o + 1], L[o + 1], uc, lc), wx[o]));
-    if (i > 0) res = fsub(res, fmul(pair_diff(uc, lc, U[o - P], L[o - P]), wy[o - P]));
-    if (i < H - 1) res = fadd(res, fmul(pair_diff(U[o + P], L[o + P], uc, lc), wy[o]));
+    if (j > 0) res = fsub(res, fmul(dpair_diff(xc, pair_val(U[o - 1], L[o - 1])), wx[o - 1]));
+    if (j < W - 1) res = fadd(res, fmul(dpair_diff(pair_val(U[o + 1], L[o + 1]), xc), wx[o]));
+    if (i > 0) res = fsub(res, fmul(dpair_diff(xc, pair_val(U[o - P], L[o - P])), wy[o - P]));
+    if (i < H - 1) res = fadd(res, fmul(dpair_diff(pair_val(U[o + P], L[o + P]), xc), wy[o]));
     return -res;
 }
 

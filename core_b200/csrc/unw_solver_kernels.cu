@@ -80,6 +80,7 @@ __global__ void k_state_init(const GridDev* __restrict__ grids, int n, UnwScalar
     s->vcount = 0; s->mean = 0; s->residual = 0; s->best_residual = INFINITY; s->rel_change = 0; s->resid_rel = 0;
     s->tol = sc.tol; s->cg_tol = sc.cg_tol; s->eps2 = sc.eps2; s->cg_max_iter = sc.cg_max_iter;
     s->cg_rel = sc.cg_rel;
+    s->refine_scale = 1.0;
     s->cg_total = 0;
     for (int i = 0; i < UNW_MAX_LOG; i++) s->cg_log[i] = 0;
     s->n_nonfinite = 0; s->n_kneg = 0; s->n_kpos = 0; s->kmin = INT_MAX; s->kmax = INT_MIN; s->hist_ok = 1; s->kmed = 0.f; s->shift = 0.f;
@@ -504,24 +505,27 @@ __global__ void __launch_bounds__(256, 4) k_head(const GridDev* __restrict__ gri
     }
     float rx[4], ry[4];
     F4 wix, wiy, bv;
+    // the centre row's pairs as float64 values, converted once and shared (dpair_diff)
+    double xv[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) xv[q] = pair_val(u.v[q], l.v[q]);
     // right neighbour of column j0+3
-    float urh = __shfl_down_sync(0xffffffffu, u.v[0], 1);
-    float url = __shfl_down_sync(0xffffffffu, l.v[0], 1);
-    if (lane == 31) { urh = ur; url = lr; }
+    double xr = __shfl_down_sync(0xffffffffu, xv[0], 1);
+    if (lane == 31) xr = pair_val(ur, lr);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const int j = j0 + q;
-        const float rh = q == 3 ? urh : u.v[q + 1], rl = q == 3 ? url : l.v[q + 1];
+        const double right = q == 3 ? xr : xv[q + 1];
         // r = grad(u) - g, last column / row: 0 - g
-        rx[q] = (j < W - 1) ? fsub(pair_diff(rh, rl, u.v[q], l.v[q]), gx.v[q]) : fsub(0.f, gx.v[q]);
-        ry[q] = hd ? fsub(pair_diff(ud.v[q], ld.v[q], u.v[q], l.v[q]), gy.v[q]) : fsub(0.f, gy.v[q]);
+        rx[q] = (j < W - 1) ? fsub(dpair_diff(right, xv[q]), gx.v[q]) : fsub(0.f, gx.v[q]);
+        ry[q] = hd ? fsub(dpair_diff(pair_val(ud.v[q], ld.v[q]), xv[q]), gy.v[q]) : fsub(0.f, gy.v[q]);
         wix.v[q] = irls_w(wx.v[q], rx[q], eps2);
         wiy.v[q] = irls_w(wy.v[q], ry[q], eps2);
     }
     float wl = __shfl_up_sync(0xffffffffu, wix.v[3], 1);
     float gl = __shfl_up_sync(0xffffffffu, gx.v[3], 1);
     if (lane == 0 && j0 > 0) {
-        const float rxl = fsub(pair_diff(u.v[0], l.v[0], ul, ll), gxl);
+        const float rxl = fsub(dpair_diff(xv[0], pair_val(ul, ll)), gxl);
         wl = irls_w(wxl, rxl, eps2);
         gl = gxl;
     }
@@ -536,7 +540,7 @@ __global__ void __launch_bounds__(256, 4) k_head(const GridDev* __restrict__ gri
         }
         if (j < W - 1) b = fsub(b, fmul(wix.v[q], gx.v[q]));
         if (hu) {
-            const float ryu = fsub(pair_diff(u.v[q], l.v[q], uu.v[q], lu.v[q]), gyu.v[q]);
+            const float ryu = fsub(dpair_diff(xv[q], pair_val(uu.v[q], lu.v[q])), gyu.v[q]);
             b = fadd(b, fmul(irls_w(wyu.v[q], ryu, eps2), gyu.v[q]));
         }
         if (hd) b = fsub(b, fmul(wiy.v[q], gy.v[q]));
@@ -546,7 +550,7 @@ __global__ void __launch_bounds__(256, 4) k_head(const GridDev* __restrict__ gri
         F4 ch, cl4;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const double c = pair_val(u.v[q], l.v[q]) - m;
+            const double c = xv[q] - m;
             split_pair(c, ch.v[q], cl4.v[q]);
             if (j0 + q < W) {
                 acc[0] += (double)fmul(rx[q], rx[q]) + (double)fmul(ry[q], ry[q]);

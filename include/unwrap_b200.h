@@ -196,8 +196,10 @@ UNW_API int unw_apply_preconditioner_mixed(const float* r, int64_t H, int64_t W,
  * phase differences, the coherence edge weights, the weighted Poisson solve
  * A(wI) u* = b (utils_unwrap2d.py:1367-1388, :1576-1581) and the per-component
  * circular-mean alignment (utils_unwrap2d.py:1694-1716).  The call first
- * refines u to u* on that frozen system, then solves the adjoint system with
- * the same DCT-preconditioned PCG, then forms the gradients.
+ * refines u to u* on that frozen system (one PCG solve from u, then float64
+ * residual-refinement passes, each correction from the same PCG), then solves
+ * the adjoint system with the same DCT-preconditioned PCG, then forms the
+ * gradients in float64.
  *   phase, weight   the forward call's inputs (device, NaN = invalid)
  *   u               the forward call's unwrapped output (device)
  *   grad_u          dL/du (device; ignored where phase is NaN)
@@ -206,8 +208,10 @@ UNW_API int unw_apply_preconditioner_mixed(const float* r, int64_t H, int64_t W,
  *                   residual norm of each solve (e.g. 1e-6)
  *   grad_phase      dL/dphase (device), 0 where phase is NaN
  *   grad_weight     dL/dweight (device) or NULL; needs weight
- *   stats           cg_iters[0] / [1]: refinement / adjoint PCG iterations,
- *                   rel_change: final relative residual of the adjoint solve
+ *   stats           cg_iters[0] / [1]: first u* / adjoint PCG iterations,
+ *                   cg_iters[2..4]: PCG iterations of the refinement passes,
+ *                   rel_change: final relative residual of the adjoint solve,
+ *                   resid_rel: float64 ||b - A u*|| / ||b|| of the final u*
  * Returns UNW_W_NUMERIC (gradients 0) when the refinement is not finite.
  */
 UNW_API size_t unw_adjoint_workspace_bytes(int64_t H, int64_t W);

@@ -210,6 +210,62 @@ class Frozen:
         gweight[r0:r1, c0:c1] = gw
         return gphase, gweight
 
+    def finite_difference_factored(self, phase, weight, grad_out, pixels, h=1e-4):
+        """Central differences of L = sum(grad_out * F) with respect to the phase at the
+        given (i, j) pixels, for grids too large for one sparse solve per evaluation.
+
+        The frozen system matrix does not depend on the phase, so it is factorised once
+        (sparse LU in symmetric mode, the first unknown pinned as in _solve).  Its
+        right-hand side is affine in one pixel's phase over [-h, h] (the wrapped
+        differences next to the pixel move by +-h and stay away from the wrap), so the
+        two evaluations share one solve: u(phase +- h e_ij) = u* +- d with
+        d = A^+ (b(phase + h e_ij) - b(phase - h e_ij)) / 2, and F(phase +- h e_ij) is the
+        full map at those u and phases (alignment included).  L(+h) - L(-h) is summed
+        from the output difference so that no two large sums are subtracted.
+        """
+        r0, r1, c0, c1 = self.crop
+        v = self.valid
+        H, W = v.shape
+        ph = np.asarray(phase, np.float64)[r0:r1, c0:c1]
+        wc = None if weight is None else np.asarray(weight, np.float64)[r0:r1, c0:c1]
+        A, b, gx, gy, wx, wy, wIx, wIy = self._system(ph, wc)
+        lu = spl.splu(A[1:, 1:].tocsc(), permc_spec="MMD_AT_PLUS_A", options=dict(SymmetricMode=True))
+
+        def solve(rhs):
+            x = np.zeros_like(rhs)
+            x[1:] = lu.solve(rhs[1:])
+            return x
+
+        def rhs_of(phc):
+            g1, g2 = self._grads(np.where(v, phc, 0.0))
+            return self.Dx.T @ (wIx * g1).ravel() + self.Dy.T @ (wIy * g2).ravel()
+
+        ustar = solve(b[:, None])[:, 0].reshape(H, W)
+        G = np.where(v, np.asarray(grad_out, np.float64)[r0:r1, c0:c1], 0.0)
+        loc = [(i - r0, j - c0) for i, j in pixels]
+        cols = []
+        for ii, jj in loc:
+            a = ph.copy()
+            a[ii, jj] += h
+            m = ph.copy()
+            m[ii, jj] -= h
+            cols.append((rhs_of(a) - rhs_of(m)) / 2)
+        D = solve(np.stack(cols, axis=1))
+        res = []
+        for k, (ii, jj) in enumerate(loc):
+            d = D[:, k].reshape(H, W)
+            adj = []
+            for sgn in (1.0, -1.0):
+                phs = ph.copy()
+                phs[ii, jj] += sgn * h
+                sp_, cp_, su, cu = self._post_terms(phs, ustar + sgn * d)
+                a_ = _wrap(np.arctan2(sp_, cp_) - np.arctan2(su, cu))
+                a_[0] = 0.0
+                adj.append(a_)
+            dout = 2 * d + (adj[0] - adj[1])[self.lab]
+            res.append(float(np.sum(G[v] * dout[v])) / (2 * h))
+        return np.array(res)
+
     def finite_difference(self, phase, weight, grad_out, pixels, h=1e-4, wrt="phase"):
         """Central differences of L = sum(grad_out * F) at the given (i, j) pixels."""
         phase = np.asarray(phase, np.float64)
@@ -231,3 +287,10 @@ class Frozen:
                 c = weight.copy(); c[i, j] -= h
                 res.append((loss(phase, a) - loss(phase, c)) / (2 * h))
         return np.array(res)
+
+
+def fd_factored_job(args):
+    """(phase, weight, u, grad_out, pixels, h) -> central differences at the pixels, from
+    a fresh Frozen map at u; a process-pool task (one grid per task)."""
+    phase, weight, u, grad_out, pixels, h = args
+    return Frozen(phase, weight, u).finite_difference_factored(phase, weight, grad_out, pixels, h=h)

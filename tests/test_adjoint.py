@@ -58,6 +58,23 @@ def test_oracle_adjoint_matches_finite_differences(kind):
         assert F.nlab >= 2
 
 
+def test_factored_finite_differences_match_plain_ones():
+    """The large-grid FD evaluator (one factorisation, one solve per pixel) against the
+    plain one (one sparse solve per map evaluation) and the oracle adjoint."""
+    p, c, _ = gen_g1(40, 48, seed=5, noise=1.0)
+    u, _ = oracle_unwrap(p, c, dtype=np.float64)
+    F = Frozen(p, c, u)
+    v = np.isfinite(p)
+    rng = np.random.default_rng(3)
+    G = np.where(v, rng.standard_normal(p.shape), np.nan)
+    pix = [tuple(x) for x in np.argwhere(v)[rng.choice(v.sum(), 12, replace=False)]]
+    a = F.finite_difference(p, c, G, pix, h=1e-5)
+    b = F.finite_difference_factored(p, c, G, pix, h=1e-4)
+    gp, _ = F.adjoint(p, c, G)
+    assert _relerr(b, a) <= 1e-6
+    assert _relerr(np.array([gp[i, j] for i, j in pix]), b) <= 1e-6
+
+
 # ------------------------------------------------------------------ GPU
 def _gpu():
     torch = pytest.importorskip("torch")
