@@ -495,7 +495,8 @@ def run_b200(args):
                            "pageable host input, pinned staging for the output"},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches // 1,
            "stack": stack, "link": link, "accuracy": accuracy, "mixed": mixed,
-           "mixed_1024": mixed_small(local) if not args.no_mixed_small else None}
+           "mixed_1024": mixed_small(local) if not args.no_mixed_small else None,
+           "diff": diff_measure(local, args.diff_large) if not args.no_diff_line else None}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
@@ -622,6 +623,66 @@ def mixed_small(local):
         row["ratio_tc_over_plain"] = round(row["mixed_tc"]["mpx_s"] / row["plain"]["mpx_s"], 4)
         out[label] = row
         del keep, ws
+        torch.cuda.empty_cache()
+    return out
+
+
+def diff_measure(local, large=False):
+    """The differentiable unwrap: a batch of 16 G1 grids of 1024^2 through
+    core_b200.irls_unwrap_2d_diff (function-default forward, adjoint at a 1e-6 relative
+    tolerance), loss = L2 distance to the true phase, forward (solve + loss) and backward
+    (frozen-weight adjoint: refinement, adjoint PCG, gradients for phase and weight) timed
+    separately with CUDA events on device-resident inputs; with large=True also one
+    20000^2 G1 grid (the adjoint re-derives the frozen system from phase, weight and u, so
+    no forward state is kept for the backward pass)."""
+    import torch
+
+    import core_b200
+    from core_b200.synthetic import gen_g1
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    cases = [("batch16_g1_1024", 16, 1024, 1, 2)] + ([("g1_20000", 1, 20000, 0, 1)] if large else [])
+    for label, count, side, warm, steps in cases:
+        grids = [gen_g1(side, side, seed=k) for k in range(count)]
+        p = torch.from_numpy(np.stack([g[0] for g in grids])).to(dev)
+        c = torch.from_numpy(np.stack([g[1] for g in grids])).to(dev)
+        t = torch.from_numpy(np.stack([g[2] for g in grids]).astype(np.float32)).to(dev)
+        del grids
+        if count == 1:
+            p, c, t = p[0], c[0], t[0]
+        torch.cuda.reset_peak_memory_stats(dev)
+
+        def step():
+            pt = p.detach().requires_grad_(True)
+            ct = c.detach().requires_grad_(True)
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            torch.cuda.synchronize()
+            e[0].record(stream)
+            u, _ = core_b200.irls_unwrap_2d_diff(pt, ct)
+            v = torch.isfinite(u)
+            loss = 0.5 * (u[v] - t[v]).pow(2).sum()
+            e[1].record(stream)
+            loss.backward()
+            e[2].record(stream)
+            torch.cuda.synchronize()
+            ok = bool(torch.isfinite(pt.grad).all()) and bool(torch.isfinite(ct.grad).all())
+            return e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), ok
+        for _ in range(warm):
+            step()
+        fw, bw, oks = [], [], []
+        for _ in range(steps):
+            a, b, ok = step()
+            fw.append(a)
+            bw.append(b)
+            oks.append(ok)
+        npx = count * side * side
+        f_ms, b_ms = float(np.median(fw)), float(np.median(bw))
+        out[label] = {"forward_ms": round(f_ms, 2), "backward_ms": round(b_ms, 2),
+                      "fwd_bwd_mpx_s": round(npx / 1e6 / ((f_ms + b_ms) / 1e3), 3), "steps": steps,
+                      "warmup": warm, "finite_gradients": all(oks),
+                      "peak_device_gb": round(torch.cuda.max_memory_allocated(dev) / 1e9, 1)}
+        del p, c, t
         torch.cuda.empty_cache()
     return out
 
@@ -799,6 +860,10 @@ def main():
                     help="with --precision mixed: column pass chosen by the autotuner, or forced")
     ap.add_argument("--no-mixed-small", action="store_true",
                     help="leave the 1024^2 mixed-precision sub-measurement out of the default line")
+    ap.add_argument("--no-diff-line", action="store_true",
+                    help="leave the differentiable-unwrap (16 x 1024^2 forward + backward) sub-measurement out")
+    ap.add_argument("--diff-large", action="store_true",
+                    help="also time forward + backward of one 20000^2 grid in the differentiable-unwrap line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -27,6 +27,7 @@ UNW_F_FIXED_ITERS = 8
 UNW_F_MIXED = 16
 UNW_F_COL_TC = 32
 UNW_F_COL_FFT = 64
+UNW_F_COL_NO_TMA = 128
 
 PROF_NAMES = ["bbox", "setup", "row_rho", "col", "row_inv", "matvec", "row_upd", "row_r0", "head", "elem", "post"]
 PROF_N = len(PROF_NAMES)

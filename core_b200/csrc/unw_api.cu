@@ -242,6 +242,7 @@ struct Shape {
     int row_p2 = 0, col_p2 = 0;   // power-of-two register-FFT paths (length), 0 = generic
     int row_bl = 0, col_bl = 0;   // Bluestein register-FFT paths (FFT length M), 0 = not used
     int col_tc = 0;               // tensor-core column pass (mixed precision), chosen by the autotuner
+    int col_p2_tma = 0;           // power-of-two column pass with the slab moved by TMA (H = 4096)
 };
 
 int elem_ctas(long long npx) {
@@ -347,6 +348,8 @@ cudaError_t L_rowi(Solver& S, int mode) {
 }
 cudaError_t L_col(Solver& S, int mode) {
     if (S.sh.col_tc) return unw_launch_col_tc(mode, S.total[KS_TC], S.s, S.dg, S.ds(KS_TC), S.n, &S.maps, S.bmaps);
+    if (S.sh.col_p2_tma)
+        return unw_launch_col_p2_tma(S.sh.col_p2, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n, S.bmaps);
     if (S.sh.col_p2) return unw_launch_col_p2(S.sh.col_p2, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n);
     if (S.sh.col_bl) return unw_launch_col_bl(S.sh.col_bl, mode, S.total[KS_COL], S.s, S.dg, S.ds(KS_COL), S.n);
     return unw_launch_col(mode, S.sh.col_T, S.sh.col_emax, S.total[KS_COL], S.sh.col_smem, S.s, S.dg, S.ds(KS_COL),
@@ -354,7 +357,43 @@ cudaError_t L_col(Solver& S, int mode) {
 }
 
 // ------------------------------------------------------------ IRLS enqueue
-int enqueue_iteration(Solver& S, int t) {
+int enqueue_pcg(Solver& S, int t, int k0, int k1);
+
+// The PCG of a single-instance solver after its start pass, in chunks of `chunk` iterations
+// until the instance's PCG has stopped or cg_max_iter is reached: a solve that stops after k
+// iterations costs about k launches of each kernel instead of cg_max_iter gated ones.
+int pcg_chunked(Solver& S, int t, int chunk) {
+    for (int k0 = 0; k0 < S.sc.cg_max_iter; k0 += chunk) {
+        const int rc = enqueue_pcg(S, t, k0, std::min(S.sc.cg_max_iter, k0 + chunk));
+        if (rc) return rc;
+        int flags[2] = {0, 0};  // cg_active, irls_active of instance 0
+        const InstState* d = S.hg[0].st;
+        CK(cudaMemcpyAsync(&flags[0], &d->cg_active, sizeof(int), cudaMemcpyDeviceToHost, S.s));
+        CK(cudaMemcpyAsync(&flags[1], &d->irls_active, sizeof(int), cudaMemcpyDeviceToHost, S.s));
+        CK(cudaStreamSynchronize(S.s));
+        if (!flags[0] || !flags[1]) break;
+    }
+    return UNW_OK;
+}
+
+// PCG iterations k0 .. k1-1 of IRLS iteration t (each kernel returns at once for an
+// instance whose PCG has stopped)
+int enqueue_pcg(Solver& S, int t, int k0, int k1) {
+    const int n = S.n;
+    cudaStream_t s = S.s;
+    for (int k = k0; k < k1; k++) {
+        PL(UNW_PROF_MATVEC, unw_launch_simple(UNW_K_MATVEC, S.total[KS_MATVEC], s, S.dg, S.ds(KS_MATVEC), n, k, S.sc));
+        PL(UNW_PROF_ROW_UPD, L_rowf(S, 2, t, k));
+        PL(UNW_PROF_COL, L_col(S, 2));
+        PL(UNW_PROF_ROW_INV, L_rowi(S, 2));
+    }
+    return UNW_OK;
+}
+
+// One IRLS iteration; with chunk > 0 the PCG runs in chunks of that many iterations with a
+// read of the instance's state between chunks (single-instance solvers with a large PCG cap:
+// the adjoint), else all cg_max_iter iterations are enqueued (graph capture).
+int enqueue_iteration(Solver& S, int t, int chunk = 0) {
     const int n = S.n;
     cudaStream_t s = S.s;
     PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_MEAN, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
@@ -363,12 +402,8 @@ int enqueue_iteration(Solver& S, int t) {
     PL(UNW_PROF_ROW_R0, L_rowf(S, 1, t, 0));
     PL(UNW_PROF_COL, L_col(S, 1));
     PL(UNW_PROF_ROW_INV, L_rowi(S, 1));
-    for (int k = 0; k < S.sc.cg_max_iter; k++) {
-        PL(UNW_PROF_MATVEC, unw_launch_simple(UNW_K_MATVEC, S.total[KS_MATVEC], s, S.dg, S.ds(KS_MATVEC), n, k, S.sc));
-        PL(UNW_PROF_ROW_UPD, L_rowf(S, 2, t, k));
-        PL(UNW_PROF_COL, L_col(S, 2));
-        PL(UNW_PROF_ROW_INV, L_rowi(S, 2));
-    }
+    const int rc = chunk > 0 ? pcg_chunked(S, t, chunk) : enqueue_pcg(S, t, 0, S.sc.cg_max_iter);
+    if (rc) return rc;
     PL(UNW_PROF_ELEM, unw_launch_simple(UNW_K_REL, S.total[KS_ELEM], s, S.dg, S.ds(KS_ELEM), n, t, S.sc));
     return UNW_OK;
 }
@@ -720,6 +755,26 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
         }
         cudaGetLastError();
     }
+    // power-of-two column pass with the slab moved by TMA: per-grid tensor maps of T (even and
+    // odd rows) in the grid's 256-byte map slot (the tensor-core pass, which uses the same slots,
+    // covers H <= 1024 only)
+    S.sh.col_p2_tma = 0;
+    if (!S.sh.col_tc && S.sh.col_p2 && unw_p2_tma_nseq(S.sh.col_p2) > 0 && !(prm->flags & UNW_F_COL_NO_TMA)) {
+        std::vector<unsigned char> hm(256 * (size_t)n + 64);
+        unsigned char* h = (unsigned char*)up((size_t)hm.data(), 64);
+        bool ok = true;
+        for (int g = 0; g < n && ok; g++) {
+            const GridDev& G = S.hg[g];
+            if (G.H > 0)
+                ok = G.col_nseq == unw_p2_tma_nseq(S.sh.col_p2) &&
+                     unw_p2_tma_maps(G.T, G.H, G.W, G.P, G.col_nseq, h + 256 * (size_t)g);
+        }
+        if (ok) {
+            S.bmaps = base + B.tcmaps + 256 * (size_t)slot;
+            CK(cudaMemcpyAsync(S.bmaps, h, 256 * (size_t)n, cudaMemcpyHostToDevice, s));
+            S.sh.col_p2_tma = 1;
+        }
+    }
     bool any_grid = false;
     for (int g = 0; g < n; g++) any_grid |= S.hg[g].H > 0;
     if ((prm->flags & UNW_F_MIXED) && (prm->flags & UNW_F_COL_TC) && !S.sh.col_tc && any_grid) {
@@ -831,6 +886,9 @@ int solve_group(const std::vector<int>& idx, const unw_grid* grids, const std::v
         if (G.H == 0) status |= UNW_S_ALL_NAN;
         else {
             status = st.status;
+            if (status & UNW_S_TC_TIMEOUT)
+                return set_err(UNW_E_CUDA, "grid %d: a TMA-staged column pass gave up waiting on its copies",
+                               idx[g]);
             if (st.n_nonfinite) { status |= UNW_S_NONFINITE_OUT; ret = UNW_W_NUMERIC; }
             else if (!st.hist_ok) return set_err(UNW_E_UNSUPPORTED, "grid %d: post-processing limits exceeded", idx[g]);
         }
@@ -1057,7 +1115,7 @@ int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_
     CK(unw_launch_adj(UNW_A_LOAD, ne, s, S.dg, S.ds(KS_ELEM), n, u, u_pitch, gu, gu_pitch, nullptr, 0, nullptr, 0));
     // 1. the frozen-weight system at u (IRLS weights and right-hand side from u), solved to
     //    the relative tolerance from u: u* in U1
-    rc = enqueue_iteration(S, 0);
+    rc = enqueue_iteration(S, 0, UNW_ADJ_CHUNK);
     if (rc) return rc;
     // 2. iterative refinement of u* on the frozen system: residual in float64 (phase
     //    differences in float64), correction by the PCG from x0 = 0, added to the pair; the
@@ -1073,12 +1131,8 @@ int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_
         CK(L_rowf(S, 1, 1, 0));
         CK(L_col(S, 1));
         CK(L_rowi(S, 1));
-        for (int c = 0; c < S.sc.cg_max_iter; c++) {
-            CK(unw_launch_simple(UNW_K_MATVEC, S.total[KS_MATVEC], s, S.dg, S.ds(KS_MATVEC), n, c, S.sc));
-            CK(L_rowf(S, 2, 1, c));
-            CK(L_col(S, 2));
-            CK(L_rowi(S, 2));
-        }
+        rc = pcg_chunked(S, 1, UNW_ADJ_CHUNK);
+        if (rc) return rc;
         CK(unw_launch_adj(UNW_A_ADDD, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0,
                           k));
     }
@@ -1100,12 +1154,8 @@ int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_
     CK(L_rowf(S, 1, 1, 0));
     CK(L_col(S, 1));
     CK(L_rowi(S, 1));
-    for (int k = 0; k < S.sc.cg_max_iter; k++) {
-        CK(unw_launch_simple(UNW_K_MATVEC, S.total[KS_MATVEC], s, S.dg, S.ds(KS_MATVEC), n, k, S.sc));
-        CK(L_rowf(S, 2, 1, k));
-        CK(L_col(S, 2));
-        CK(L_rowi(S, 2));
-    }
+    rc = pcg_chunked(S, 1, UNW_ADJ_CHUNK);
+    if (rc) return rc;
     // 5. gradients
     CK(unw_launch_adj(UNW_A_GRAD, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, gph, gph_pitch, gw,
                       gw_pitch));

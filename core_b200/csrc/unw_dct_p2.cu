@@ -184,6 +184,9 @@ __device__ __forceinline__ void rowi_store4(const GridDev& G, int i, int j, floa
     }
 }
 
+#ifndef UNW_ROWI_STAGED
+#define UNW_ROWI_STAGED 1
+#endif
 template <int N, int MODE>
 __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const GridDev* __restrict__ grids,
                                                                          const int* __restrict__ starts, int n) {
@@ -214,6 +217,42 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
             if (has1) asm volatile("prefetch.global.L2 [%0];" ::"l"(ra + P + c));
         }
     }
+#if UNW_ROWI_STAGED
+    // the row pair's T values: all eight 16-byte loads of a thread issued together, then
+    // (Y_a[k], Y_b[k]) into sm[pad16(k)]
+    float4 ya[N / (4 * T)], yb[N / (4 * T)];
+#pragma unroll
+    for (int m = 0; m < N / (4 * T); m++) {
+        const int c4 = t + m * T;
+        ya[m] = ld4f(Ta, 4 * c4);
+        yb[m] = has1 ? ld4f(Tb, 4 * c4) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();  // previous row pair's reads of sm are done
+#pragma unroll
+    for (int m = 0; m < N / (4 * T); m++) {
+        const int k = 4 * (t + m * T);
+#pragma unroll
+        for (int c = 0; c < 4; c++) sm[pad16(k + c)] = make_float2(f4get(ya[m], c), f4get(yb[m], c));
+    }
+    __syncthreads();
+    // DCT-III pre-twiddle in place, one frequency pair (k, N-k) per step (both outputs read
+    // only this pair): V'_k = conj(w_k) (Y_k - i Y_{N-k}), Y_N = 0; store conj(C')
+    for (int k = t; k <= N / 2; k += T) {
+        const int km = N - k;
+        const float2 yk = sm[pad16(k)];
+        const float2 ym = k ? sm[pad16(km)] : make_float2(0.f, 0.f);
+        const float2 wk = cconj(__ldg(&dw[k]));
+        const float2 Pa = cmul(wk, make_float2(yk.x, -ym.x));
+        const float2 Pb = cmul(wk, make_float2(yk.y, -ym.y));
+        if (k && km != k) {
+            const float2 wm = cconj(__ldg(&dw[km]));
+            const float2 Qa = cmul(wm, make_float2(ym.x, -yk.x));
+            const float2 Qb = cmul(wm, make_float2(ym.y, -yk.y));
+            sm[pad16(km)] = cconj(make_float2(Qa.x - Qb.y, Qa.y + Qb.x));
+        }
+        sm[pad16(k)] = cconj(make_float2(Pa.x - Pb.y, Pa.y + Pb.x));
+    }
+#else
     __syncthreads();  // previous row pair's reads of sm are done
     // DCT-III pre-twiddle: V'_k = conj(w_k) (Y_k - i Y_{N-k}), Y_N = 0; store conj(C')
     for (int c4 = t; c4 < N / 4; c4 += T) {
@@ -237,8 +276,37 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
             sm[pad16(k)] = cconj(make_float2(Pa.x - Pb.y, Pa.y + Pb.x));
         }
     }
+#endif
     __syncthreads();
     smem_fft<N>(sm, t, G.prow.fft.tw);
+#if UNW_ROWI_STAGED
+    if (MODE == 2) {
+        // p = z + beta p: the thread's p loads (L2-prefetched above) all issued before the
+        // first use
+        float4 pa[N / (4 * T)], pb[N / (4 * T)];
+#pragma unroll
+        for (int m = 0; m < N / (4 * T); m++) {
+            const size_t o = (size_t)i0 * P + 4 * (t + m * T);
+            pa[m] = ld4f(G.p0, o);
+            pb[m] = has1 ? ld4f(G.p0, o + P) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int m = 0; m < N / (4 * T); m++) {
+            const int j = 4 * (t + m * T);
+            float za[4], zb[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const float2 v = sm[pad16(mk_pos(j + c, N))];
+                za[c] = fadd(fmul(f4get(pa[m], c), beta), v.x);
+                zb[c] = fadd(fmul(f4get(pb[m], c), beta), -v.y);
+            }
+            const size_t o = (size_t)i0 * P + j;
+            st4f(G.p0, o, make_float4(za[0], za[1], za[2], za[3]));
+            if (has1) st4f(G.p0, o + P, make_float4(zb[0], zb[1], zb[2], zb[3]));
+        }
+        continue;
+    }
+#endif
     for (int c4 = t; c4 < N / 4; c4 += T) {
         const int j = 4 * c4;
         float za[4], zb[4];

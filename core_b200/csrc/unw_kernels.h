@@ -128,8 +128,15 @@ enum {
 cudaError_t unw_launch_post(int which, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
                             int n, const UnwScalars& sc, const GridDev* host_grids);
 
+// power-of-two column pass with the slab moved by TMA (unw_dct_p2_tma.cu), H = 4096
+int unw_p2_tma_nseq(int N);
+bool unw_p2_tma_maps(const float* T, int H, int W, int P, int nseq, void* out);
+cudaError_t unw_launch_col_p2_tma(int N, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
+                                  int n, const void* maps);
+
 // frozen-weight adjoint (KS_ELEM shapes except REARM)
 #define UNW_ADJ_REFINE 3    // refinement passes of u* (each stops early below 1e-13 residual)
+#define UNW_ADJ_CHUNK 8     // adjoint PCG iterations enqueued between reads of the instance state
 enum {
     UNW_A_LOAD = 0,     // forward output and dL/dout into the crop
     UNW_A_LSUM,         // per-component sum of dL/dout

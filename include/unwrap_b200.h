@@ -69,6 +69,9 @@ typedef struct unw_params {
 #define UNW_F_COL_TC 32     /* with UNW_F_MIXED: always the tensor-core column pass (else
                                UNW_E_UNSUPPORTED), no autotuning                             */
 #define UNW_F_COL_FFT 64    /* with UNW_F_MIXED: always the float32 FFT column pass          */
+#define UNW_F_COL_NO_TMA 128 /* power-of-two column pass at H = 4096 with plain loads
+                               and stores instead of TMA copies of the column slab (the same
+                               arithmetic and bits; for comparison)                         */
 
 /* Kernel families timed under UNW_F_PROFILE (index into unw_stats.prof_*). */
 enum {
@@ -106,8 +109,9 @@ typedef struct unw_stats {
 #define UNW_S_REVERTED           2   /* reverted to the best iterate             */
 #define UNW_S_NONFINITE_OUT      4   /* non-finite output: NaN result            */
 #define UNW_S_ALL_NAN            8   /* input all NaN                            */
-#define UNW_S_TC_TIMEOUT        16   /* a tensor-core pass gave up waiting on its
-                                        pipeline (bounded wait); result not valid */
+#define UNW_S_TC_TIMEOUT        16   /* a TMA-staged column pass (tensor-core or
+                                        power-of-two) gave up waiting on its copies
+                                        (bounded wait); result not valid        */
 
 /* One grid of a batched solve (unw_solve_batch).  Pitches are in elements. */
 typedef struct unw_grid {

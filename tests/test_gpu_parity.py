@@ -454,6 +454,19 @@ def test_graph_launches_equal_direct_launches(shape):
     assert s1["cg_iters_total"] == s2["cg_iters_total"]
 
 
+@pytest.mark.parametrize("shape", [(4096, 1000), (4096, 3), (4096, 333)])
+def test_tma_column_pass_equals_plain_loads(shape):
+    # at H = 4096 the column pass moves its slab by TMA unless UNW_F_COL_NO_TMA is set; the
+    # arithmetic is the same, so both must give identical bits (and no timeout status)
+    p, c, _ = gen_g1(*shape, seed=11)
+    u1, c1, s1 = _solve_flags(p, c, 0)
+    u2, c2, s2 = _solve_flags(p, c, _lib.UNW_F_COL_NO_TMA)
+    np.testing.assert_array_equal(u1.view(np.uint32), u2.view(np.uint32))
+    np.testing.assert_array_equal(c1, c2)
+    assert s1["irls_iters"] == s2["irls_iters"] and s1["cg_iters_total"] == s2["cg_iters_total"]
+    assert not s1["status"] & _lib.UNW_S_TC_TIMEOUT
+
+
 def test_fixed_iters_runs_every_iteration():
     # tol = cg_tol = 0: only the numerical breaks can end an iteration early
     from oracle.irls_oracle import OracleStats
