@@ -451,6 +451,18 @@ def run_b200(args):
         pos = [mine.index(m) for m in (0, 1, 2) if m in mine]
         s_val, s_t, s_iters, s_out, _ = stack_measure(sph, swt, 3, 2, world, local, s_npx, keep_out=pos)
         m_val, m_t, _, _, m_paths = stack_measure(sph, swt, 1, 2, world, local, s_npx, flags=_lib.UNW_F_MIXED)
+        # equal work per pixel on both workloads: 3 IRLS x 20 PCG iterations, every stop test off
+        f_val, f_t, _, _, _ = stack_measure(sph, swt, 1, 2, world, local, s_npx, flags=_lib.UNW_F_FIXED_ITERS,
+                                            over={"max_iter": 3})
+        for _ in range(2):
+            solve(_lib.UNW_F_FIXED_ITERS, max_iter=3)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(3):
+            solve(_lib.UNW_F_FIXED_ITERS, max_iter=3)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        g_fixed = npx / 1e6 / (ev0.elapsed_time(ev1) / 1e3 / 3)
         stack = {"value": round(s_val, 3), "unit": UNIT, "ms_per_step": round(s_t * 1e3, 1), "steps": 2,
                  "warmup": 3, "grids": 64, "total_mpx": round(s_npx / 1e6, 1),
                  "workload": "64 G1 grids, rows U[1500,2600] x cols U[4000,7000], noise U[0.2,0.8], "
@@ -461,6 +473,12 @@ def run_b200(args):
                            "tensor_core_grids": int(sum(m_paths)),
                            "note": "every stack grid has more than 1024 rows, so the mixed form keeps the "
                                    "float32 FFT column pass (the tensor-core pass covers H <= 1024)"},
+                 "fixed_iters_3x20": {"stack_mpx_s": round(f_val, 3), "stack_ms_per_step": round(f_t * 1e3, 1),
+                                      "single_grid_mpx_s": round(g_fixed, 3),
+                                      "note": "both workloads at exactly 3 IRLS x 20 PCG iterations (stop tests "
+                                              "off): per-pixel work is equal, so the two Mpx/s compare the "
+                                              "launch shapes (Bluestein stack grids vs the power-of-two 4096^2 "
+                                              "grid) rather than iteration counts"},
                  "accuracy": stack_accuracy({mine[k]: s_out[k] for k in s_out}, sph, mine) if rank == 0 else None}
         del sph, swt
 
@@ -755,7 +773,7 @@ def link_measure(local, steps, warmup):
                         "linksize 5, linkcount 30, IRLS-style labels given"}
 
 
-def stack_measure(phases, weights, warmup, steps, world, local, npx_all, flags=0, keep_out=()):
+def stack_measure(phases, weights, warmup, steps, world, local, npx_all, flags=0, keep_out=(), over=None):
     """Batched solves of this rank's grids, inputs resident in HBM: (Mpx/s over the whole
     stack, seconds per step (max over ranks), per-grid IRLS counts, {position: u} of the
     positions in `keep_out` copied to the host, per-grid column paths).  `flags` are extra
@@ -783,7 +801,7 @@ def stack_measure(phases, weights, warmup, steps, world, local, npx_all, flags=0
     ws = torch.empty(lib.unw_batch_workspace_bytes(n, Hs, Ws) if n else 1, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     sts = (_lib.UnwStats * max(n, 1))()
-    prm = make_params(**FN)
+    prm = make_params(**dict(FN, **(over or {})))
     prm.flags |= flags
 
     def solve():

@@ -7,9 +7,10 @@ oracle's (and with finite differences) on the same inputs and the same
 forward solution.
 
 Tolerances, relative to the largest gradient: oracle vs finite differences
-1e-4 (h = 1e-5 phase, 1e-6 weight); CUDA (float32 PCG solves to 1e-6 relative
-residual) vs the oracle 1e-4 for dL/dphase and dL/dweight, and vs finite
-differences 1e-4.
+1e-4 (h = 1e-5 phase, 1e-6 weight); oracle vs torch autograd through the unrolled
+float64 PCG solve of the same map (oracle/adjoint_unrolled.py) 1e-6; CUDA
+(float32 PCG solves to 1e-6 relative residual, float64 refinement of u*) vs the
+oracle, vs the unrolled autograd and vs finite differences 1e-4.
 """
 import numpy as np
 import pytest
@@ -75,6 +76,24 @@ def test_factored_finite_differences_match_plain_ones():
     assert _relerr(np.array([gp[i, j] for i, j in pix]), b) <= 1e-6
 
 
+@pytest.mark.parametrize("kind", ["full", "nan", "split"])
+def test_unrolled_fp64_autograd_matches_oracle_adjoint(kind):
+    """torch autograd through the unrolled float64 PCG solve of the same frozen map
+    (oracle/adjoint_unrolled.py) against the oracle's hand-written adjoint (exact sparse
+    solves): two independent derivations of dL/dphase and dL/dweight."""
+    from oracle.adjoint_unrolled import UnrolledMap
+    p, c = _case(kind, H=40, W=48, seed=5)
+    u, _ = oracle_unwrap(p, c)
+    v = np.isfinite(p)
+    rng = np.random.default_rng(2)
+    G = np.where(v, rng.standard_normal(p.shape), np.nan)
+    op, ow = Frozen(p, c, u).adjoint(p, c, G)
+    gp, gw, iters = UnrolledMap(p, c, u).gradients(p, c, G)
+    assert 0 < iters < 20000
+    assert _relerr(gp, op) <= 1e-6
+    assert _relerr(gw, ow) <= 1e-6
+
+
 # ------------------------------------------------------------------ GPU
 def _gpu():
     torch = pytest.importorskip("torch")
@@ -106,6 +125,28 @@ def test_cuda_adjoint_matches_oracle(kind):
     pix = [tuple(x) for x in np.argwhere(v)[rng.choice(v.sum(), 16, replace=False)]]
     fdp = F.finite_difference(p, c, G, pix, h=1e-5)
     assert _relerr(np.array([gph[i, j] for i, j in pix]), fdp) <= 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["full", "nan", "split"])
+def test_cuda_adjoint_matches_unrolled_fp64_autograd(kind):
+    """The CUDA adjoint against torch autograd through an unrolled float64 PCG solve of
+    the frozen map (no hand-written adjoint on the reference side), within 1e-4 of the
+    largest gradient."""
+    torch = _gpu()
+    import core_b200
+    from oracle.adjoint_unrolled import UnrolledMap
+    p, c = _case(kind, H=40, W=48, seed=5)
+    dev = torch.device("cuda", 0)
+    u, _ = core_b200.irls_unwrap_2d(p, c)
+    v = np.isfinite(p)
+    rng = np.random.default_rng(4)
+    G = np.where(v, rng.standard_normal(p.shape), np.nan).astype(np.float32)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+    gph, gw, st = core_b200.irls_adjoint(T(p), T(c), T(u), T(np.nan_to_num(G)), cg_max_iter=3000, cg_tol=1e-6)
+    ap, aw, _ = UnrolledMap(p, c, u).gradients(p, c, G)
+    assert _relerr(gph.cpu().numpy(), ap) <= 1e-4
+    assert _relerr(gw.cpu().numpy(), aw) <= 1e-4
 
 
 @pytest.mark.gpu
