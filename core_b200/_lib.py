@@ -86,6 +86,14 @@ class UnwGrid(C.Structure):
                 ("out_cc_pitch", C.c_int64)]
 
 
+class UnwAdjGrid(C.Structure):
+    _fields_ = [("phase", C.c_void_p), ("phase_pitch", C.c_int64), ("weight", C.c_void_p),
+                ("weight_pitch", C.c_int64), ("H", C.c_int64), ("W", C.c_int64),
+                ("u", C.c_void_p), ("u_pitch", C.c_int64), ("grad_u", C.c_void_p), ("grad_u_pitch", C.c_int64),
+                ("grad_phase", C.c_void_p), ("grad_phase_pitch", C.c_int64),
+                ("grad_weight", C.c_void_p), ("grad_weight_pitch", C.c_int64)]
+
+
 # every symbol include/unwrap_b200.h declares, with its ctypes signature
 SIGNATURES = {
     "unw_abi_version": (C.c_int, []),
@@ -107,6 +115,9 @@ SIGNATURES = {
                                                  C.c_void_p, C.c_size_t, C.c_void_p]),
     "unw_apply_preconditioner_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "unw_adjoint_workspace_bytes": (C.c_size_t, [C.c_int64, C.c_int64]),
+    "unw_adjoint_batch_workspace_bytes": (C.c_size_t, [C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "unw_adjoint_batch": (C.c_int, [C.c_int32, C.POINTER(UnwAdjGrid), C.POINTER(UnwParams), C.c_void_p,
+                                    C.c_size_t, C.POINTER(UnwStats), C.c_void_p]),
     "unw_goldstein_workspace_bytes": (C.c_size_t, [C.c_int64, C.c_int64, C.c_int32, C.c_int32]),
     "unw_goldstein_c64": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
                                     C.c_int32, C.c_int32, C.c_float, C.c_void_p, C.c_int64, C.c_void_p,

@@ -1,7 +1,8 @@
 """Differentiable unwrap: a torch.autograd.Function over the B200 solver.
 
 The forward pass is `irls_unwrap_2d` on CUDA tensors.  The backward pass calls
-`unw_adjoint_f32`: gradients of the unwrap with the forward solution's IRLS
+`unw_adjoint_f32` (one grid) or `unw_adjoint_batch` (a (B, H, W) batch, one launch
+sequence for all grids): gradients of the unwrap with the forward solution's IRLS
 scale, valid mask, components and median 2-pi shift held fixed (the frozen
 final IRLS system of insardev/insardev/utils_unwrap2d.py:1529-1626 and the
 alignment of :1667-1716), through an implicit adjoint solve with the same
@@ -40,11 +41,45 @@ def irls_adjoint(phase, weight, u, grad_u, *, cg_max_iter=1000, cg_tol=1e-6, eps
                                  gw.data_ptr() if gw is not None else None, W, ws.data_ptr(), ws.numel(),
                                  C.byref(st), torch.cuda.current_stream(dev).cuda_stream)
     _lib.check(rc, "unw_adjoint_f32")
-    stats = {"refine_cg_iters": int(st.cg_iters[0]), "adjoint_cg_iters": int(st.cg_iters[1]),
-             "refine_pass_cg_iters": [int(st.cg_iters[2 + k]) for k in range(3)],
-             "refine_rel_residual": float(st.resid_rel),
-             "adjoint_rel_residual": float(st.rel_change), "status": int(st.status), "numeric_warning": rc == 1}
-    return gph, gw, stats
+    return gph, gw, _adj_stats(st, rc)
+
+
+def _adj_stats(st, rc):
+    return {"refine_cg_iters": int(st.cg_iters[0]), "adjoint_cg_iters": int(st.cg_iters[1]),
+            "refine_pass_cg_iters": [int(st.cg_iters[2 + k]) for k in range(3)],
+            "refine_rel_residual": float(st.resid_rel),
+            "adjoint_rel_residual": float(st.rel_change), "status": int(st.status), "numeric_warning": rc == 1}
+
+
+def irls_adjoint_batch(phase, weight, u, grad_u, *, cg_max_iter=1000, cg_tol=1e-6, epsilon=1e-2,
+                       need_weight=True):
+    """`irls_adjoint` for a (B, H, W) batch through one `unw_adjoint_batch` call.
+
+    Returns (grad_phase (B, H, W), grad_weight (B, H, W) or None, list of per-grid stats).
+    """
+    torch = _torch()
+    lib = _lib.load()
+    dev = phase.device
+    nb, H, W = (int(x) for x in phase.shape)
+    f32 = lambda t: t.detach().to(device=dev, dtype=torch.float32).contiguous()
+    ph, uu, gu = f32(phase), f32(u), f32(grad_u)
+    wt = f32(weight) if weight is not None else None
+    gph = torch.empty((nb, H, W), dtype=torch.float32, device=dev)
+    gw = torch.empty((nb, H, W), dtype=torch.float32, device=dev) if (wt is not None and need_weight) else None
+    grids = (_lib.UnwAdjGrid * nb)()
+    for b in range(nb):
+        grids[b] = _lib.UnwAdjGrid(ph[b].data_ptr(), W, wt[b].data_ptr() if wt is not None else None, W, H, W,
+                                   uu[b].data_ptr(), W, gu[b].data_ptr(), W, gph[b].data_ptr(), W,
+                                   gw[b].data_ptr() if gw is not None else None, W)
+    Hs, Ws = (C.c_int64 * nb)(*([H] * nb)), (C.c_int64 * nb)(*([W] * nb))
+    ws = torch.empty(lib.unw_adjoint_batch_workspace_bytes(nb, Hs, Ws), dtype=torch.uint8, device=dev)
+    prm = make_params(cg_max_iter=cg_max_iter, cg_tol=cg_tol, epsilon=epsilon)
+    sts = (_lib.UnwStats * nb)()
+    with torch.cuda.device(dev):
+        rc = lib.unw_adjoint_batch(nb, grids, C.byref(prm), ws.data_ptr(), ws.numel(), sts,
+                                   torch.cuda.current_stream(dev).cuda_stream)
+    _lib.check(rc, "unw_adjoint_batch")
+    return gph, gw, [_adj_stats(sts[b], rc) for b in range(nb)]
 
 
 def _make_function():
@@ -73,13 +108,9 @@ def _make_function():
             phase, weight, u = ctx.saved_tensors
             need_w = ctx.has_weight and ctx.needs_input_grad[1]
             if phase.ndim == 3:
-                gphs, gws = [], []
-                for b in range(phase.shape[0]):
-                    w = weight[b] if ctx.has_weight else None
-                    gph, gw, _ = irls_adjoint(phase[b], w, u[b], grad_u[b], need_weight=need_w, **ctx.akw)
-                    gphs.append(gph)
-                    gws.append(gw)
-                return torch.stack(gphs), (torch.stack(gws) if need_w else None), None, None
+                w = weight if ctx.has_weight else None
+                gph, gw, _ = irls_adjoint_batch(phase, w, u, grad_u, need_weight=need_w, **ctx.akw)
+                return gph, (gw if need_w else None), None, None
             w = weight if ctx.has_weight else None
             gph, gw, _ = irls_adjoint(phase, w, u, grad_u, need_weight=need_w, **ctx.akw)
             return gph, gw, None, None
@@ -95,7 +126,7 @@ def irls_unwrap_2d_diff(phase, weight=None, max_iter=50, tol=1e-3, cg_max_iter=2
     """`irls_unwrap_2d` on CUDA tensors with gradients for phase and weight.
 
     phase (and weight): one (H, W) grid or a (B, H, W) batch (one batched forward
-    solve; one adjoint solve per grid in the backward pass).
+    solve; one batched adjoint in the backward pass).
     Returns (u, conncomp); u carries autograd history (conncomp does not).
     adjoint_cg_max_iter / adjoint_cg_tol control the backward pass's PCG solves
     (tolerance relative to each solve's initial residual).

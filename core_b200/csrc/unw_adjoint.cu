@@ -35,8 +35,7 @@
 
 // u (forward output, NaN outside the valid pixels) -> iterate pair (U0, L0 = 0) on the crop, NaN -> 0;
 // dL/dout -> z (unused by the solver), 0 at invalid pixels.
-__global__ void k_adj_load(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n,
-                           const float* __restrict__ u, long long up, const float* __restrict__ gu, long long gp) {
+__global__ void k_adj_load(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
     const int g = find_grid(starts, n, blockIdx.x);
     const GridDev& G = grids[g];
     const int local = blockIdx.x - starts[g];
@@ -44,8 +43,8 @@ __global__ void k_adj_load(const GridDev* __restrict__ grids, const int* __restr
     UNW_ROWS_LOOP(G, local, nct) {
         const size_t o = (size_t)i * G.P + j;
         const long long gi = (long long)(G.r0 + i), gj = (long long)(G.c0 + j);
-        const float uv = u[gi * up + gj];
-        const float gv = gu[gi * gp + gj];
+        const float uv = G.a_u[gi * G.a_u_pitch + gj];
+        const float gv = G.a_gu[gi * G.a_gu_pitch + gj];
         const bool v = G.valid[o] != 0;
         G.U0[o] = (v && isfinite(uv)) ? uv : 0.f;
         G.L0[o] = 0.f;
@@ -244,8 +243,7 @@ __global__ void k_adj_rearm(const GridDev* __restrict__ grids, int n) {
 }
 
 // gradients into the caller's full grids (the crop region; the host zeroes the rest)
-__global__ void k_adj_grad(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n,
-                           float* __restrict__ gph, long long gpp, float* __restrict__ gw, long long gwp) {
+__global__ void k_adj_grad(const GridDev* __restrict__ grids, const int* __restrict__ starts, int n) {
     const int g = find_grid(starts, n, blockIdx.x);
     const GridDev& G = grids[g];
     const int local = blockIdx.x - starts[g];
@@ -253,6 +251,9 @@ __global__ void k_adj_grad(const GridDev* __restrict__ grids, const int* __restr
     const size_t cap = (size_t)G.lab_cap;
     const int nlab = G.st->n_labels;
     const int H = G.H, W = G.W, P = G.P;
+    float* __restrict__ gph = G.a_gph;
+    float* __restrict__ gw = G.a_gw;
+    const long long gpp = G.a_gph_pitch, gwp = G.a_gw_pitch;
     const float* __restrict__ lam = G.D;   // the adjoint PCG's x - x0 with x0 = 0
     UNW_ROWS_LOOP(G, local, nct) {
         const size_t o = (size_t)i * P + j;
@@ -302,16 +303,14 @@ __global__ void k_adj_grad(const GridDev* __restrict__ grids, const int* __restr
     }
 }
 
-cudaError_t unw_launch_adj(int which, int nblk, cudaStream_t s, const GridDev* gd, const int* starts, int n,
-                           const float* a, long long ap, const float* b, long long bp, float* c, long long cp,
-                           float* d, long long dp, int k) {
+cudaError_t unw_launch_adj(int which, int nblk, cudaStream_t s, const GridDev* gd, const int* starts, int n, int k) {
     if (nblk <= 0) return cudaSuccess;
     switch (which) {
-        case UNW_A_LOAD: k_adj_load<<<nblk, 256, 0, s>>>(gd, starts, n, a, ap, b, bp); break;
+        case UNW_A_LOAD: k_adj_load<<<nblk, 256, 0, s>>>(gd, starts, n); break;
         case UNW_A_LSUM: k_adj_lsum<<<nblk, 256, 0, s>>>(gd, starts, n); break;
         case UNW_A_RHS: k_adj_rhs<<<nblk, 256, 0, s>>>(gd, starts, n); break;
         case UNW_A_REARM: k_adj_rearm<<<(n + 63) / 64, 64, 0, s>>>(gd, n); break;
-        case UNW_A_GRAD: k_adj_grad<<<nblk, 256, 0, s>>>(gd, starts, n, c, cp, d, dp); break;
+        case UNW_A_GRAD: k_adj_grad<<<nblk, 256, 0, s>>>(gd, starts, n); break;
         case UNW_A_REFINE:
             if (k) k_adj_refine<1><<<nblk, 256, 0, s>>>(gd, starts, n);
             else k_adj_refine<0><<<nblk, 256, 0, s>>>(gd, starts, n);

@@ -363,15 +363,20 @@ int enqueue_pcg(Solver& S, int t, int k0, int k1);
 // until the instance's PCG has stopped or cg_max_iter is reached: a solve that stops after k
 // iterations costs about k launches of each kernel instead of cg_max_iter gated ones.
 int pcg_chunked(Solver& S, int t, int chunk) {
+    const int n = S.n;
+    std::vector<int> flags(2 * (size_t)n);  // cg_active, irls_active per instance
     for (int k0 = 0; k0 < S.sc.cg_max_iter; k0 += chunk) {
         const int rc = enqueue_pcg(S, t, k0, std::min(S.sc.cg_max_iter, k0 + chunk));
         if (rc) return rc;
-        int flags[2] = {0, 0};  // cg_active, irls_active of instance 0
-        const InstState* d = S.hg[0].st;
-        CK(cudaMemcpyAsync(&flags[0], &d->cg_active, sizeof(int), cudaMemcpyDeviceToHost, S.s));
-        CK(cudaMemcpyAsync(&flags[1], &d->irls_active, sizeof(int), cudaMemcpyDeviceToHost, S.s));
+        for (int g = 0; g < n; g++) {
+            const InstState* d = S.hg[g].st;
+            CK(cudaMemcpyAsync(&flags[2 * g], &d->cg_active, sizeof(int), cudaMemcpyDeviceToHost, S.s));
+            CK(cudaMemcpyAsync(&flags[2 * g + 1], &d->irls_active, sizeof(int), cudaMemcpyDeviceToHost, S.s));
+        }
         CK(cudaStreamSynchronize(S.s));
-        if (!flags[0] || !flags[1]) break;
+        bool any = false;
+        for (int g = 0; g < n; g++) any |= S.hg[g].H > 0 && flags[2 * g] && flags[2 * g + 1];
+        if (!any) break;
     }
     return UNW_OK;
 }
@@ -1025,94 +1030,70 @@ int solve_batch(int n, const unw_grid* grids, const unw_params* prm, void* ws, s
 }
 
 // ------------------------------------------------------------ adjoint
-// Workspace of the adjoint: the solver layout of one grid plus a separate
-// post-processing region, since the component labels and sums must live
+// Workspace of the adjoint: the solver layout of the batch plus a separate
+// post-processing region per grid, since the component labels and sums must live
 // next to the frozen weights (which the forward solve lets them overlay).
 struct AdjLayout {
     BatchLayout B;
-    size_t parent, lab, csum, adj, ccount, remap, total;
+    std::vector<size_t> parent, lab, csum, adj, ccount, remap;
+    size_t total;
 };
 
-AdjLayout adjoint_layout(long long H, long long W) {
+AdjLayout adjoint_layout(int n, const long long* H, const long long* W) {
     AdjLayout A;
-    A.B = batch_layout(1, &H, &W);
-    const long long cap = A.B.g[0].lab_cap;
+    A.B = batch_layout(n, H, W);
     size_t o = up(A.B.total - ALIGN, ALIGN);
     auto take = [&](size_t bytes) { size_t r = o; o = up(o + bytes, ALIGN); return r; };
-    A.parent = take(sizeof(int) * (size_t)(H * W));
-    A.lab = take(sizeof(int) * (size_t)(H * W));
-    A.csum = take(sizeof(double) * 4 * (size_t)cap);
-    A.adj = take(sizeof(double) * (size_t)cap);
-    A.ccount = take(sizeof(int) * (size_t)cap);
-    A.remap = take(sizeof(int) * (size_t)cap);
+    for (int g = 0; g < n; g++) {
+        const long long cap = A.B.g[g].lab_cap;
+        A.parent.push_back(take(sizeof(int) * (size_t)(H[g] * W[g])));
+        A.lab.push_back(take(sizeof(int) * (size_t)(H[g] * W[g])));
+        A.csum.push_back(take(sizeof(double) * 4 * (size_t)cap));
+        A.adj.push_back(take(sizeof(double) * (size_t)cap));
+        A.ccount.push_back(take(sizeof(int) * (size_t)cap));
+        A.remap.push_back(take(sizeof(int) * (size_t)cap));
+    }
     A.total = o + ALIGN;
     return A;
 }
 
-int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_t weight_pitch, int64_t H, int64_t W,
-            const unw_params* prm, const float* u, int64_t u_pitch, const float* gu, int64_t gu_pitch, float* gph,
-            int64_t gph_pitch, float* gw, int64_t gw_pitch, void* ws, size_t ws_bytes, unw_stats* stats,
-            cudaStream_t s) {
-    if (!phase || !u || !gu || !gph) return set_err(UNW_E_ARG, "null pointer");
-    if (H <= 0 || W <= 0) return set_err(UNW_E_ARG, "bad shape %lld x %lld", (long long)H, (long long)W);
-    if (H * W >= (1LL << 31)) return set_err(UNW_E_UNSUPPORTED, "too many pixels");
-    if (phase_pitch < W || u_pitch < W || gu_pitch < W || gph_pitch < W || (weight && weight_pitch < W) ||
-        (gw && gw_pitch < W))
-        return set_err(UNW_E_ARG, "pitch smaller than width");
-    if (gw && !weight) return set_err(UNW_E_ARG, "grad_weight needs weight");
-    int rc = validate_params(prm);
-    if (rc) return rc;
-    if (prm->cg_max_iter < 1 || !(prm->cg_tol > 0.f))
-        return set_err(UNW_E_ARG, "adjoint needs cg_max_iter >= 1 and a relative cg_tol > 0");
-    if (!ws) return set_err(UNW_E_ARG, "workspace is NULL");
-    const AdjLayout A = adjoint_layout(H, W);
-    char* base = (char*)up((size_t)ws, ALIGN);
-    if ((size_t)(base - (char*)ws) + A.total - ALIGN > ws_bytes)
-        return set_err(UNW_E_WORKSPACE, "workspace %zu bytes < %zu needed", ws_bytes, A.total);
-    if (stats) memset(stats, 0, sizeof(unw_stats));
-    CK(cudaMemset2DAsync(gph, sizeof(float) * gph_pitch, 0, sizeof(float) * W, H, s));
-    if (gw) CK(cudaMemset2DAsync(gw, sizeof(float) * gw_pitch, 0, sizeof(float) * W, H, s));
-
-    // bounding box of the valid pixels, as in the forward solve
-    const BatchLayout& B = A.B;
-    int* dbbox = (int*)(base + B.bbox);
-    CK(unw_launch_bbox(phase, phase_pitch, (int)H, (int)W, (int*)(base + B.rowany), (int*)(base + B.colany), dbbox,
-                       s));
-    std::vector<int> bbox(4);
-    CK(cudaMemcpyAsync(bbox.data(), dbbox, sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    if (bbox[1] <= bbox[0] || bbox[3] <= bbox[2]) return UNW_OK;  // all NaN: zero gradients
-
-    unw_grid q{};
-    q.phase = phase;
-    q.phase_pitch = phase_pitch;
-    q.weight = weight;
-    q.weight_pitch = weight_pitch;
-    q.H = H;
-    q.W = W;
+// One launch group of the adjoint: every kernel covers the group's grids; each grid's
+// PCG solves stop on their own tolerance.
+int adjoint_group(const std::vector<int>& idx, const unw_adj_grid* grids, const std::vector<unw_grid>& q,
+                  const std::vector<int>& bbox, const unw_params* prm, char* base, const AdjLayout& A,
+                  unw_stats* stats, cudaStream_t s, int slot, int soff) {
     unw_params pa = *prm;
     pa.max_iter = 1;
     pa.flags = 0;
     Solver S;
-    rc = prepare(S, std::vector<int>{0}, &q, bbox, &pa, base, B, s, false, 0, 0);
+    int rc = prepare(S, idx, q.data(), bbox, &pa, base, A.B, s, false, slot, soff);
     if (rc) return rc;
     S.sc.cg_tol = 0.f;            // replaced by cg_rel * ||r0|| at each PCG start
     S.sc.cg_rel = prm->cg_tol;
-    {
-        GridDev& G = S.hg[0];
-        G.parent = (int*)(base + A.parent);
-        G.lab = (int*)(base + A.lab);
-        G.csum = (double*)(base + A.csum);
-        G.adj = (double*)(base + A.adj);
-        G.ccount = (int*)(base + A.ccount);
-        G.remap = (int*)(base + A.remap);
-        CK(cudaMemcpyAsync(S.dg, S.hg.data(), sizeof(GridDev), cudaMemcpyHostToDevice, s));
+    const int n = (int)idx.size();
+    for (int g = 0; g < n; g++) {
+        GridDev& G = S.hg[g];
+        const int j = idx[g];
+        G.parent = (int*)(base + A.parent[j]);
+        G.lab = (int*)(base + A.lab[j]);
+        G.csum = (double*)(base + A.csum[j]);
+        G.adj = (double*)(base + A.adj[j]);
+        G.ccount = (int*)(base + A.ccount[j]);
+        G.remap = (int*)(base + A.remap[j]);
+        G.a_u = grids[j].u;
+        G.a_u_pitch = grids[j].u_pitch;
+        G.a_gu = grids[j].grad_u;
+        G.a_gu_pitch = grids[j].grad_u_pitch;
+        G.a_gph = grids[j].grad_phase;
+        G.a_gph_pitch = grids[j].grad_phase_pitch;
+        G.a_gw = grids[j].grad_weight;
+        G.a_gw_pitch = grids[j].grad_weight_pitch;
     }
-    const int n = 1;
+    CK(cudaMemcpyAsync(S.dg, S.hg.data(), sizeof(GridDev) * (size_t)n, cudaMemcpyHostToDevice, s));
     const int ne = S.total[KS_ELEM];
     CK(unw_launch_simple(UNW_K_STATE_INIT, 1, s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
     CK(unw_launch_simple(UNW_K_SETUP, ne, s, S.dg, S.ds(KS_ELEM), n, 0, S.sc));
-    CK(unw_launch_adj(UNW_A_LOAD, ne, s, S.dg, S.ds(KS_ELEM), n, u, u_pitch, gu, gu_pitch, nullptr, 0, nullptr, 0));
+    CK(unw_launch_adj(UNW_A_LOAD, ne, s, S.dg, S.ds(KS_ELEM), n));
     // 1. the frozen-weight system at u (IRLS weights and right-hand side from u), solved to
     //    the relative tolerance from u: u* in U1
     rc = enqueue_iteration(S, 0, UNW_ADJ_CHUNK);
@@ -1122,19 +1103,16 @@ int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_
     //    last REFINE only measures the residual of the final u*.  Before the post pipeline,
     //    which sets u* to NaN outside the valid pixels (its shift is 0 here: no median ran)
     for (int k = 0; k <= UNW_ADJ_REFINE; k++) {
-        CK(unw_launch_adj(UNW_A_REARM, 1, s, S.dg, nullptr, n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
-        CK(unw_launch_adj(UNW_A_REFINE, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr,
-                          0, 0));
+        CK(unw_launch_adj(UNW_A_REARM, 1, s, S.dg, nullptr, n));
+        CK(unw_launch_adj(UNW_A_REFINE, ne, s, S.dg, S.ds(KS_ELEM), n, 0));
         if (k == UNW_ADJ_REFINE) break;
-        CK(unw_launch_adj(UNW_A_REFINE, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr,
-                          0, 1));
+        CK(unw_launch_adj(UNW_A_REFINE, ne, s, S.dg, S.ds(KS_ELEM), n, 1));
         CK(L_rowf(S, 1, 1, 0));
         CK(L_col(S, 1));
         CK(L_rowi(S, 1));
         rc = pcg_chunked(S, 1, UNW_ADJ_CHUNK);
         if (rc) return rc;
-        CK(unw_launch_adj(UNW_A_ADDD, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0,
-                          k));
+        CK(unw_launch_adj(UNW_A_ADDD, ne, s, S.dg, S.ds(KS_ELEM), n, k));
     }
     // 3. components of the valid mask
     const int nt = S.total[KS_NKIND];
@@ -1146,43 +1124,125 @@ int adjoint(const float* phase, int64_t phase_pitch, const float* weight, int64_
     CK(unw_launch_post(UNW_P_ACCUM, ne, s, S.dg, S.ds(KS_ELEM), n, S.sc, S.hg.data()));
     // 4. adjoint right-hand side through the alignment, then lambda = A^+ G' (x0 = 0 in U0/L0,
     //    lambda accumulated in D)
-    CK(cudaMemsetAsync(S.hg[0].adj, 0, sizeof(double) * (size_t)S.hg[0].lab_cap, s));
-    CK(cudaMemsetAsync(S.hg[0].csum, 0, sizeof(double) * 4 * (size_t)S.hg[0].lab_cap, s));
-    CK(unw_launch_adj(UNW_A_LSUM, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
-    CK(unw_launch_adj(UNW_A_RHS, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
-    CK(unw_launch_adj(UNW_A_REARM, 1, s, S.dg, nullptr, n, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, 0));
+    for (int g = 0; g < n; g++) {
+        CK(cudaMemsetAsync(S.hg[g].adj, 0, sizeof(double) * (size_t)S.hg[g].lab_cap, s));
+        CK(cudaMemsetAsync(S.hg[g].csum, 0, sizeof(double) * 4 * (size_t)S.hg[g].lab_cap, s));
+    }
+    CK(unw_launch_adj(UNW_A_LSUM, ne, s, S.dg, S.ds(KS_ELEM), n));
+    CK(unw_launch_adj(UNW_A_RHS, ne, s, S.dg, S.ds(KS_ELEM), n));
+    CK(unw_launch_adj(UNW_A_REARM, 1, s, S.dg, nullptr, n));
     CK(L_rowf(S, 1, 1, 0));
     CK(L_col(S, 1));
     CK(L_rowi(S, 1));
     rc = pcg_chunked(S, 1, UNW_ADJ_CHUNK);
     if (rc) return rc;
     // 5. gradients
-    CK(unw_launch_adj(UNW_A_GRAD, ne, s, S.dg, S.ds(KS_ELEM), n, nullptr, 0, nullptr, 0, gph, gph_pitch, gw,
-                      gw_pitch));
+    CK(unw_launch_adj(UNW_A_GRAD, ne, s, S.dg, S.ds(KS_ELEM), n));
     std::vector<InstState> hs;
     rc = read_states(S, hs);
     if (rc) return rc;
-    const InstState& st = hs[0];
-    if (stats) {
-        unw_stats& o = *stats;
-        o.irls_iters = 1;
-        o.cg_iters[0] = st.cg_log[0];
-        o.cg_iters[1] = st.cg_iter;
-        o.cg_iters_last = st.cg_iter;
-        o.cg_iters_total = st.cg_log[0] + st.cg_iter;
-        for (int k = 0; k < UNW_ADJ_REFINE; k++) {
-            o.cg_iters[2 + k] = st.cg_log[2 + k];
-            o.cg_iters_total += st.cg_log[2 + k];
+    int ret = UNW_OK;
+    for (int g = 0; g < n; g++) {
+        const InstState& st = hs[g];
+        if (st.status & UNW_S_TC_TIMEOUT)
+            return set_err(UNW_E_CUDA, "grid %d: a TMA-staged column pass gave up waiting on its copies", idx[g]);
+        if (stats) {
+            unw_stats& o = stats[idx[g]];
+            o.irls_iters = 1;
+            o.cg_iters[0] = st.cg_log[0];
+            o.cg_iters[1] = st.cg_iter;
+            o.cg_iters_last = st.cg_iter;
+            o.cg_iters_total = st.cg_log[0] + st.cg_iter;
+            for (int k = 0; k < UNW_ADJ_REFINE; k++) {
+                o.cg_iters[2 + k] = st.cg_log[2 + k];
+                o.cg_iters_total += st.cg_log[2 + k];
+            }
+            o.resid_rel = st.resid_rel;
+            o.n_labels = st.n_labels;
+            o.status = st.status;
+            // relative residual of the adjoint solve (cg_tol = cg_rel * ||r0||)
+            o.rel_change = st.cg_tol > 0.f ? st.rnorm * (double)prm->cg_tol / (double)st.cg_tol : 0.0;
+            for (int k = 0; k < 4; k++) o.bbox[k] = bbox[4 * idx[g] + k];
         }
-        o.resid_rel = st.resid_rel;
-        o.n_labels = st.n_labels;
-        o.status = st.status;
-        // relative residual of the adjoint solve (cg_tol = cg_rel * ||r0||)
-        o.rel_change = st.cg_tol > 0.f ? st.rnorm * (double)prm->cg_tol / (double)st.cg_tol : 0.0;
-        for (int k = 0; k < 4; k++) o.bbox[k] = bbox[k];
+        if (!st.irls_active) ret = UNW_W_NUMERIC;  // non-finite refinement: this grid's gradients are zero
     }
-    if (!st.irls_active) return UNW_W_NUMERIC;  // non-finite refinement: gradients are zero
-    return UNW_OK;
+    return ret;
+}
+
+int adjoint_batch(int n, const unw_adj_grid* grids, const unw_params* prm, void* ws, size_t ws_bytes,
+                  unw_stats* stats, cudaStream_t s) {
+    if (n <= 0 || !grids) return set_err(UNW_E_ARG, "empty batch");
+    int rc = validate_params(prm);
+    if (rc) return rc;
+    if (prm->cg_max_iter < 1 || !(prm->cg_tol > 0.f))
+        return set_err(UNW_E_ARG, "adjoint needs cg_max_iter >= 1 and a relative cg_tol > 0");
+    std::vector<long long> H0(n), W0(n);
+    std::vector<unw_grid> q(n);
+    for (int g = 0; g < n; g++) {
+        const unw_adj_grid& a = grids[g];
+        if (!a.phase || !a.u || !a.grad_u || !a.grad_phase) return set_err(UNW_E_ARG, "grid %d: null pointer", g);
+        if (a.H <= 0 || a.W <= 0) return set_err(UNW_E_ARG, "grid %d: bad shape %lld x %lld", g, a.H, a.W);
+        if (a.H * a.W >= (1LL << 31)) return set_err(UNW_E_UNSUPPORTED, "grid %d: too many pixels", g);
+        if (a.phase_pitch < a.W || a.u_pitch < a.W || a.grad_u_pitch < a.W || a.grad_phase_pitch < a.W ||
+            (a.weight && a.weight_pitch < a.W) || (a.grad_weight && a.grad_weight_pitch < a.W))
+            return set_err(UNW_E_ARG, "grid %d: pitch smaller than width", g);
+        if (a.grad_weight && !a.weight) return set_err(UNW_E_ARG, "grid %d: grad_weight needs weight", g);
+        H0[g] = a.H;
+        W0[g] = a.W;
+        unw_grid& x = q[g];
+        memset(&x, 0, sizeof(x));
+        x.phase = a.phase;
+        x.phase_pitch = a.phase_pitch;
+        x.weight = a.weight;
+        x.weight_pitch = a.weight_pitch;
+        x.H = a.H;
+        x.W = a.W;
+    }
+    if (!ws) return set_err(UNW_E_ARG, "workspace is NULL");
+    const AdjLayout A = adjoint_layout(n, H0.data(), W0.data());
+    char* base = (char*)up((size_t)ws, ALIGN);
+    if ((size_t)(base - (char*)ws) + A.total - ALIGN > ws_bytes)
+        return set_err(UNW_E_WORKSPACE, "workspace %zu bytes < %zu needed", ws_bytes, A.total);
+    if (stats)
+        for (int g = 0; g < n; g++) memset(&stats[g], 0, sizeof(unw_stats));
+    for (int g = 0; g < n; g++) {
+        const unw_adj_grid& a = grids[g];
+        CK(cudaMemset2DAsync(a.grad_phase, sizeof(float) * a.grad_phase_pitch, 0, sizeof(float) * a.W, a.H, s));
+        if (a.grad_weight)
+            CK(cudaMemset2DAsync(a.grad_weight, sizeof(float) * a.grad_weight_pitch, 0, sizeof(float) * a.W, a.H, s));
+    }
+    // bounding boxes of the valid pixels, as in the forward solve
+    const BatchLayout& B = A.B;
+    int* rowany = (int*)(base + B.rowany);
+    int* colany = (int*)(base + B.colany);
+    int* dbbox = (int*)(base + B.bbox);
+    {
+        long long ro = 0, co = 0;
+        for (int g = 0; g < n; g++) {
+            CK(unw_launch_bbox(grids[g].phase, grids[g].phase_pitch, (int)H0[g], (int)W0[g], rowany + ro,
+                               colany + co, dbbox + 4 * g, s));
+            ro += H0[g];
+            co += W0[g];
+        }
+    }
+    std::vector<int> bbox(4 * n);
+    CK(cudaMemcpyAsync(bbox.data(), dbbox, sizeof(int) * 4 * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    // launch groups of the non-empty grids (an all-NaN grid has zero gradients), one after another
+    std::map<std::array<int, 4>, std::vector<int>> groups;
+    for (int g = 0; g < n; g++) {
+        const int h = bbox[4 * g + 1] - bbox[4 * g], w = bbox[4 * g + 3] - bbox[4 * g + 2];
+        if (h > 0 && w > 0) groups[group_key(h, w)].push_back(g);
+    }
+    int ret = UNW_OK, slot = 0, soff = 0;
+    for (auto& kv : groups) {
+        rc = adjoint_group(kv.second, grids, q, bbox, prm, base, A, stats, s, slot, soff);
+        if (rc < 0) return rc;
+        if (rc == UNW_W_NUMERIC) ret = rc;
+        slot += (int)kv.second.size();
+        soff += (KS_NKIND + 1) * ((int)kv.second.size() + 1);
+    }
+    return ret;
 }
 
 // Full-grid, dense-pitch descriptor over caller arrays for the operator entry points.
@@ -1261,9 +1321,22 @@ int unw_solve_batch(int32_t n, const unw_grid* grids, const unw_params* params, 
     return solve_batch(n, grids, params, workspace, workspace_bytes, stats, (cudaStream_t)cuda_stream);
 }
 
-size_t unw_adjoint_workspace_bytes(int64_t H, int64_t W) {
-    if (H <= 0 || W <= 0) return 0;
-    return adjoint_layout(H, W).total;
+size_t unw_adjoint_batch_workspace_bytes(int32_t n, const int64_t* H, const int64_t* W) {
+    if (n <= 0 || !H || !W) return 0;
+    std::vector<long long> h(n), w(n);
+    for (int g = 0; g < n; g++) {
+        if (H[g] <= 0 || W[g] <= 0) return 0;
+        h[g] = H[g];
+        w[g] = W[g];
+    }
+    return adjoint_layout(n, h.data(), w.data()).total;
+}
+
+size_t unw_adjoint_workspace_bytes(int64_t H, int64_t W) { return unw_adjoint_batch_workspace_bytes(1, &H, &W); }
+
+int unw_adjoint_batch(int32_t n, const unw_adj_grid* grids, const unw_params* params, void* workspace,
+                      size_t workspace_bytes, unw_stats* stats, void* cuda_stream) {
+    return adjoint_batch(n, grids, params, workspace, workspace_bytes, stats, (cudaStream_t)cuda_stream);
 }
 
 int unw_adjoint_f32(const float* phase, int64_t phase_pitch, const float* weight, int64_t weight_pitch, int64_t H,
@@ -1271,9 +1344,22 @@ int unw_adjoint_f32(const float* phase, int64_t phase_pitch, const float* weight
                     int64_t grad_u_pitch, float* grad_phase, int64_t grad_phase_pitch, float* grad_weight,
                     int64_t grad_weight_pitch, void* workspace, size_t workspace_bytes, unw_stats* stats,
                     void* cuda_stream) {
-    return adjoint(phase, phase_pitch, weight, weight_pitch, H, W, params, u, u_pitch, grad_u, grad_u_pitch,
-                   grad_phase, grad_phase_pitch, grad_weight, grad_weight_pitch, workspace, workspace_bytes, stats,
-                   (cudaStream_t)cuda_stream);
+    unw_adj_grid g;
+    g.phase = phase;
+    g.phase_pitch = phase_pitch;
+    g.weight = weight;
+    g.weight_pitch = weight_pitch;
+    g.H = H;
+    g.W = W;
+    g.u = u;
+    g.u_pitch = u_pitch;
+    g.grad_u = grad_u;
+    g.grad_u_pitch = grad_u_pitch;
+    g.grad_phase = grad_phase;
+    g.grad_phase_pitch = grad_phase_pitch;
+    g.grad_weight = grad_weight;
+    g.grad_weight_pitch = grad_weight_pitch;
+    return adjoint_batch(1, &g, params, workspace, workspace_bytes, stats, (cudaStream_t)cuda_stream);
 }
 
 int unw_setup_gradients(const float* phase, const float* weight, int64_t H, int64_t W, float* gx, float* gy,

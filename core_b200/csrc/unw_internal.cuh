@@ -122,6 +122,11 @@ struct GridDev {
     int lab_cap;
     int* tilecnt;               // roots per scan tile
     int ntiles;
+    // frozen-weight adjoint: the caller's full grids (forward output, dL/du in; gradients out)
+    const float* a_u;  long long a_u_pitch;
+    const float* a_gu; long long a_gu_pitch;
+    float* a_gph;      long long a_gph_pitch;
+    float* a_gw;       long long a_gw_pitch;    // may be null
 };
 
 // ---------------------------------------------------------------- helpers

@@ -147,5 +147,4 @@ enum {
     UNW_A_ADDD          // u* += correction (pass k)
 };
 cudaError_t unw_launch_adj(int which, int nblk, cudaStream_t s, const GridDev* gd, const int* starts, int n,
-                           const float* a, long long ap, const float* b, long long bp, float* c, long long cp,
-                           float* d, long long dp, int k = 0);
+                           int k = 0);

@@ -230,6 +230,32 @@ UNW_API int unw_adjoint_f32(const float* phase, int64_t phase_pitch,
                             unw_stats* stats, void* cuda_stream);
 
 /*
+ * Batched form of unw_adjoint_f32: the adjoints of n grids (each with its own
+ * forward output and dL/du) in one launch sequence per launch shape, every
+ * kernel covering all grids of its group and each grid's PCG solves stopping on
+ * their own tolerance.  Same arguments per grid as unw_adjoint_f32 (pitches in
+ * elements); stats is an array of n (or NULL).  No reference counterpart (the
+ * reference has no differentiable path); the autograd function of
+ * core_b200.irls_unwrap_2d_diff uses it for (B, H, W) batches.  Returns
+ * UNW_W_NUMERIC when the refinement of any grid is not finite (that grid's
+ * gradients are 0).
+ */
+typedef struct unw_adj_grid {
+    const float* phase;   int64_t phase_pitch;
+    const float* weight;  int64_t weight_pitch;       /* may be NULL */
+    int64_t H, W;
+    const float* u;       int64_t u_pitch;            /* forward output */
+    const float* grad_u;  int64_t grad_u_pitch;       /* dL/du */
+    float* grad_phase;    int64_t grad_phase_pitch;
+    float* grad_weight;   int64_t grad_weight_pitch;  /* may be NULL; needs weight */
+} unw_adj_grid;
+
+UNW_API size_t unw_adjoint_batch_workspace_bytes(int32_t n, const int64_t* H, const int64_t* W);
+UNW_API int unw_adjoint_batch(int32_t n, const unw_adj_grid* grids, const unw_params* params,
+                              void* workspace, size_t workspace_bytes, unw_stats* stats,
+                              void* cuda_stream);
+
+/*
  * Goldstein adaptive phase filter on one grid.  Replaces the GPU path of
  * insardev's filter, goldstein_pytorch (utils_goldstein.py:157-330, dispatched
  * from Batch.py:2023-2027): psize_y x psize_x patches at half-patch steps,

@@ -150,6 +150,32 @@ def test_cuda_adjoint_matches_unrolled_fp64_autograd(kind):
 
 
 @pytest.mark.gpu
+def test_adjoint_batch_matches_single_calls():
+    """unw_adjoint_batch over grids of one shape with different masks (one split into
+    two components, one all NaN) against one unw_adjoint_f32 call per grid."""
+    torch = _gpu()
+    import core_b200
+    dev = torch.device("cuda", 0)
+    cases = [_case("full", H=40, W=48, seed=5), _case("nan", H=40, W=48, seed=6), _case("split", H=40, W=48, seed=7)]
+    allnan = (np.full((40, 48), np.nan, np.float32), np.full((40, 48), 0.5, np.float32))
+    cases.append(allnan)
+    ps = np.stack([c[0] for c in cases]).astype(np.float32)
+    cs = np.stack([c[1] for c in cases]).astype(np.float32)
+    us = np.stack([core_b200.irls_unwrap_2d(p, c)[0] for p, c in cases]).astype(np.float32)
+    rng = np.random.default_rng(9)
+    G = np.where(np.isfinite(us), rng.standard_normal(us.shape), 0.0).astype(np.float32)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+    gph, gw, sts = core_b200.irls_adjoint_batch(T(ps), T(cs), T(us), T(G))
+    assert len(sts) == 4
+    for b in range(4):
+        g1, w1, s1 = core_b200.irls_adjoint(T(ps[b]), T(cs[b]), T(us[b]), T(G[b]))
+        np.testing.assert_array_equal(gph[b].cpu().numpy(), g1.cpu().numpy())
+        np.testing.assert_array_equal(gw[b].cpu().numpy(), w1.cpu().numpy())
+        assert sts[b]["adjoint_cg_iters"] == s1["adjoint_cg_iters"]
+    assert (gph[3] == 0).all() and (gw[3] == 0).all()
+
+
+@pytest.mark.gpu
 def test_autograd_function_backward():
     torch = _gpu()
     import core_b200
