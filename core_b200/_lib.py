@@ -28,6 +28,7 @@ UNW_F_MIXED = 16
 UNW_F_COL_TC = 32
 UNW_F_COL_FFT = 64
 UNW_F_COL_NO_TMA = 128
+UNW_F_COL_TMA = 256
 
 PROF_NAMES = ["bbox", "setup", "row_rho", "col", "row_inv", "matvec", "row_upd", "row_r0", "head", "elem", "post"]
 PROF_N = len(PROF_NAMES)
@@ -51,7 +52,7 @@ class UnwStats(C.Structure):
                 ("bbox", C.c_int32 * 4), ("rel_change", C.c_double), ("best_residual", C.c_double),
                 ("k_median", C.c_double), ("cg_iters", C.c_int32 * 64),
                 ("prof_ms", C.c_float * 16), ("prof_launches", C.c_int32 * 16),
-                ("col_path", C.c_int32), ("tune_ms", C.c_float * 2), ("pad_", C.c_int32),
+                ("col_path", C.c_int32), ("tune_ms", C.c_float * 2), ("col_tma", C.c_int32),
                 ("resid_rel", C.c_double)]
 
     def as_dict(self):
@@ -62,7 +63,8 @@ class UnwStats(C.Structure):
                     rel_change=self.rel_change, best_residual=self.best_residual,
                     k_median=self.k_median, cg_iters=list(self.cg_iters[:n]),
                     prof_ms=list(self.prof_ms[:PROF_N]), prof_launches=list(self.prof_launches[:PROF_N]),
-                    col_path=self.col_path, tune_ms=list(self.tune_ms), resid_rel=self.resid_rel)
+                    col_path=self.col_path, tune_ms=list(self.tune_ms), col_tma=self.col_tma,
+                    resid_rel=self.resid_rel)
 
 
 UNW_LINK_C_LINE = 1

@@ -242,7 +242,7 @@ struct Shape {
     int row_p2 = 0, col_p2 = 0;   // power-of-two register-FFT paths (length), 0 = generic
     int row_bl = 0, col_bl = 0;   // Bluestein register-FFT paths (FFT length M), 0 = not used
     int col_tc = 0;               // tensor-core column pass (mixed precision), chosen by the autotuner
-    int col_p2_tma = 0;           // power-of-two column pass with the slab moved by TMA (H = 4096)
+    int col_p2_tma = 0;           // power-of-two column pass with the slab moved by TMA (H 2048 / 4096)
 };
 
 int elem_ctas(long long npx) {
@@ -504,6 +504,45 @@ std::array<int, 4> group_key(int H, int W) {
         k[2] = 0; k[3] = cT * 64 + hp.emax;
     }
     return k;
+}
+
+// Autotuner of the power-of-two column pass at H = 2048 / 4096: times the pass with the
+// slab moved by TMA against the plain-load pass on the group's own buffers (DCT
+// initial-solve mode; two warm-up and three timed launches of each on the solve stream)
+// and returns 1 when TMA is faster.  Both give the same bits, so the choice changes only
+// the time.  Cached per device, H and the group's total width for the life of the
+// process; it runs before any graph capture.
+int autotune_tma(Solver& S, int H, int Wsum) {
+    static std::mutex mu;
+    static std::map<std::array<int, 3>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const std::array<int, 3> key{dev, H, Wsum};
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    cudaEvent_t e[4];
+    for (auto& x : e) cudaEventCreate(&x);
+    bool ok = true;
+    for (int tma = 0; tma < 2; tma++) {
+        S.sh.col_p2_tma = tma;
+        for (int r = 0; r < 2; r++) ok &= L_col(S, 0) == cudaSuccess;
+        cudaEventRecord(e[2 * tma], S.s);
+        for (int r = 0; r < 3; r++) ok &= L_col(S, 0) == cudaSuccess;
+        cudaEventRecord(e[2 * tma + 1], S.s);
+    }
+    float t_plain = 0.f, t_tma = 0.f;
+    int res = 1;
+    if (ok && cudaEventSynchronize(e[3]) == cudaSuccess && cudaEventElapsedTime(&t_plain, e[0], e[1]) == cudaSuccess &&
+        cudaEventElapsedTime(&t_tma, e[2], e[3]) == cudaSuccess)
+        res = t_tma < t_plain ? 1 : 0;
+    cudaGetLastError();
+    for (auto& x : e) cudaEventDestroy(x);
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = res;
+    return res;
 }
 
 // Autotuner of the mixed-precision form: times the FFT column pass against the
@@ -778,6 +817,11 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
             S.bmaps = base + B.tcmaps + 256 * (size_t)slot;
             CK(cudaMemcpyAsync(S.bmaps, h, 256 * (size_t)n, cudaMemcpyHostToDevice, s));
             S.sh.col_p2_tma = 1;
+            if (!(prm->flags & UNW_F_COL_TMA)) {
+                int Wsum = 0;
+                for (int g = 0; g < n; g++) Wsum += S.hg[g].W;
+                S.sh.col_p2_tma = autotune_tma(S, S.sh.col_p2, Wsum);
+            }
         }
     }
     bool any_grid = false;
@@ -914,6 +958,7 @@ int solve_group(const std::vector<int>& idx, const unw_grid* grids, const std::v
             o.k_median = st.kmed;
             for (int i = 0; i < 64 && i < UNW_MAX_LOG; i++) o.cg_iters[i] = G.H ? st.cg_log[i] : 0;
             o.col_path = S.sh.col_tc;
+            o.col_tma = S.sh.col_p2_tma;
             o.tune_ms[0] = S.tune.ms_fft;
             o.tune_ms[1] = S.tune.ms_tc;
             o.resid_rel = st.resid_rel;

@@ -1,12 +1,13 @@
 // Column pass of the power-of-two DCT preconditioner with the column slab moved by TMA
-// (H = 4096): the column DCT-II, the -1/lambda scaling and the column DCT-III
+// (H = 2048 and 4096): the column DCT-II, the -1/lambda scaling and the column DCT-III
 // (utils_unwrap2d.py:1390-1403, the column half of dct_2d/idct_2d at :1316-1365), the
 // same arithmetic as k_col_p2 in unw_dct_p2.cu, so the result is bit-identical.
 //
 // What changes is how the slab (2*NSEQ columns x H rows of T) reaches the registers.  A
-// row of the slab is only 16 bytes (NSEQ = 2 column pairs), so a warp's plain loads and
-// stores touch 16 rows each: 16 L1 wavefronts per request, which made the L1 data pipe
-// the busiest unit of the pass (59% of peak, 60% of its wavefronts from these accesses).  Here one thread issues 2-D TMA copies of the slab into shared memory and
+// row of the slab is only 16 (NSEQ = 2 column pairs) or 32 (NSEQ = 4) bytes, so a warp's
+// plain loads and stores touch 16 (8) rows each: one L1 wavefront per row, which at
+// H = 4096 made the L1 data pipe the busiest unit of the pass (59% of peak, 60% of its
+// wavefronts from these accesses).  Here one thread issues 2-D TMA copies of the slab into shared memory and
 // back: the even rows and the odd rows through two tensor maps (row strides 2P), so that
 // Makhoul's reordering of the DCT-II (FFT position m holds row 2m for m < H/2 and row
 // 2H-1-2m above) becomes position m of the even half or position H-1-m of the odd half:
@@ -194,13 +195,13 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, ct_min_blocks<N / 16 * NSEQ>())
     }
 }
 
-// Two column pairs per CTA, as the plain-load pass at this length.  Measured on B200
-// (CUDA-event time per column pass, bit-identical results): H = 4096, W = 4096: 92.4 us
-// against 101.8 us with plain loads; W = 1000: 35.7 / 35.3 us.  At H = 2048 (four pairs per
-// CTA, 32-byte rows) the plain loads were faster (2048 x 2048: 34.8 / 31.4 us), so the TMA
-// pass is used at H = 4096 only.
+// Column pairs per CTA: those of the plain-load pass at the same length (two at H = 4096,
+// 16-byte rows; four at H = 2048, 32-byte rows).  Which of the two passes is faster depends
+// on the shape (measured on B200, CUDA-event time per column pass, bit-identical results:
+// 4096 x 4096 92.4 us TMA / 101.8 us plain, 4096 x 1000 35.7 / 35.3, 2048 x 2048 34.8 / 31.4),
+// so the solver's autotuner times both per shape and keeps the faster.
 template <int N>
-constexpr int ct_nseq() { return 2; }
+constexpr int ct_nseq() { return N == 2048 ? 4 : 2; }
 
 template <int N>
 cudaError_t ct_launch(int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* st, int n,
@@ -236,7 +237,13 @@ PFN_cuTensorMapEncodeTiled_v12000 ct_encode_fn() {
 }  // namespace
 
 // Column sequences (pairs) per CTA of the TMA column pass; 0 where it does not apply.
-int unw_p2_tma_nseq(int N) { return N == 4096 ? ct_nseq<4096>() : 0; }
+int unw_p2_tma_nseq(int N) {
+    switch (N) {
+        case 2048: return ct_nseq<2048>();
+        case 4096: return ct_nseq<4096>();
+        default: return 0;
+    }
+}
 
 // Two tensor maps (even rows, odd rows) of the float32 H x W array T with a row pitch of
 // P floats, box 2*nseq columns x 256 rows, no swizzle; reads beyond W are zero-filled and
@@ -263,5 +270,9 @@ cudaError_t unw_launch_col_p2_tma(int N, int mode, int nblk, cudaStream_t s, con
                                   int n, const void* maps) {
     if (nblk <= 0) return cudaSuccess;
     const CUtensorMap* m = (const CUtensorMap*)maps;
-    return N == 4096 ? ct_launch<4096>(mode, nblk, s, gd, starts, n, m) : cudaErrorInvalidValue;
+    switch (N) {
+        case 2048: return ct_launch<2048>(mode, nblk, s, gd, starts, n, m);
+        case 4096: return ct_launch<4096>(mode, nblk, s, gd, starts, n, m);
+        default: return cudaErrorInvalidValue;
+    }
 }

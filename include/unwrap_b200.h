@@ -69,9 +69,11 @@ typedef struct unw_params {
 #define UNW_F_COL_TC 32     /* with UNW_F_MIXED: always the tensor-core column pass (else
                                UNW_E_UNSUPPORTED), no autotuning                             */
 #define UNW_F_COL_FFT 64    /* with UNW_F_MIXED: always the float32 FFT column pass          */
-#define UNW_F_COL_NO_TMA 128 /* power-of-two column pass at H = 4096 with plain loads
-                               and stores instead of TMA copies of the column slab (the same
-                               arithmetic and bits; for comparison)                         */
+#define UNW_F_COL_NO_TMA 128 /* power-of-two column pass at H = 2048 / 4096 with plain
+                               loads and stores, never TMA copies of the column slab (the
+                               same arithmetic and bits); by default an autotuner times both
+                               per shape on the first call and keeps the faster               */
+#define UNW_F_COL_TMA 256    /* always the TMA-staged column pass where it applies           */
 
 /* Kernel families timed under UNW_F_PROFILE (index into unw_stats.prof_*). */
 enum {
@@ -98,7 +100,7 @@ typedef struct unw_stats {
     int32_t col_path;       /* column pass used: 0 float32 FFT, 1 tensor cores  */
     float tune_ms[2];       /* autotuner: FFT / tensor-core column pass, ms per
                                launch (UNW_F_MIXED, 0 when not timed)          */
-    int32_t pad_;
+    int32_t col_tma;        /* 1: the power-of-two column pass moved its slab by TMA */
     double resid_rel;       /* ||b - A u|| / ||b|| of the final weighted system
                                in float64 (UNW_F_MIXED; 0 otherwise): the error
                                of the result against an exact solve of the last

@@ -454,13 +454,17 @@ def test_graph_launches_equal_direct_launches(shape):
     assert s1["cg_iters_total"] == s2["cg_iters_total"]
 
 
-@pytest.mark.parametrize("shape", [(4096, 1000), (4096, 3), (4096, 333)])
+@pytest.mark.parametrize("shape", [(4096, 1000), (4096, 3), (4096, 333), (2048, 777), (2048, 2048)])
 def test_tma_column_pass_equals_plain_loads(shape):
-    # at H = 4096 the column pass moves its slab by TMA unless UNW_F_COL_NO_TMA is set; the
-    # arithmetic is the same, so both must give identical bits (and no timeout status)
+    # at H = 2048 / 4096 the column pass can move its slab by TMA (forced here; by default an
+    # autotuner picks the faster per shape); the arithmetic is the same as the plain-load
+    # pass, so both must give identical bits (and no timeout status)
     p, c, _ = gen_g1(*shape, seed=11)
-    u1, c1, s1 = _solve_flags(p, c, 0)
+    u1, c1, s1 = _solve_flags(p, c, _lib.UNW_F_COL_TMA)
     u2, c2, s2 = _solve_flags(p, c, _lib.UNW_F_COL_NO_TMA)
+    assert s1["col_tma"] == 1 and s2["col_tma"] == 0
+    u3, c3, s3 = _solve_flags(p, c, 0)
+    np.testing.assert_array_equal(u1.view(np.uint32), u3.view(np.uint32))
     np.testing.assert_array_equal(u1.view(np.uint32), u2.view(np.uint32))
     np.testing.assert_array_equal(c1, c2)
     assert s1["irls_iters"] == s2["irls_iters"] and s1["cg_iters_total"] == s2["cg_iters_total"]
