@@ -449,7 +449,9 @@ def run_b200(args):
     if not args.no_stack_line:
         mine, sph, swt, s_npx = stack_grids(64, rank, world)
         pos = [mine.index(m) for m in (0, 1, 2) if m in mine]
-        s_val, s_t, s_iters, s_out, _ = stack_measure(sph, swt, 3, 2, world, local, s_npx, keep_out=pos)
+        s_prof = {}
+        s_val, s_t, s_iters, s_out, _ = stack_measure(sph, swt, 3, 2, world, local, s_npx, keep_out=pos,
+                                                      profile_out=s_prof)
         m_val, m_t, _, _, m_paths = stack_measure(sph, swt, 1, 2, world, local, s_npx, flags=_lib.UNW_F_MIXED)
         # equal work per pixel on both workloads: 3 IRLS x 20 PCG iterations, every stop test off
         f_val, f_t, _, _, _ = stack_measure(sph, swt, 1, 2, world, local, s_npx, flags=_lib.UNW_F_FIXED_ITERS,
@@ -473,6 +475,9 @@ def run_b200(args):
                            "tensor_core_grids": int(sum(m_paths)),
                            "note": "every stack grid has more than 1024 rows, so the mixed form keeps the "
                                    "float32 FFT column pass (the tensor-core pass covers H <= 1024)"},
+                 "kernels": {"note": "per-launch CUDA-event times of one separately profiled batched solve of "
+                                     "this rank's grids (launch groups one after another; the timed steps run "
+                                     "them concurrently)", **s_prof},
                  "fixed_iters_3x20": {"stack_mpx_s": round(f_val, 3), "stack_ms_per_step": round(f_t * 1e3, 1),
                                       "single_grid_mpx_s": round(g_fixed, 3),
                                       "note": "both workloads at exactly 3 IRLS x 20 PCG iterations (stop tests "
@@ -773,7 +778,8 @@ def link_measure(local, steps, warmup):
                         "linksize 5, linkcount 30, IRLS-style labels given"}
 
 
-def stack_measure(phases, weights, warmup, steps, world, local, npx_all, flags=0, keep_out=(), over=None):
+def stack_measure(phases, weights, warmup, steps, world, local, npx_all, flags=0, keep_out=(), over=None,
+                  profile_out=None):
     """Batched solves of this rank's grids, inputs resident in HBM: (Mpx/s over the whole
     stack, seconds per step (max over ranks), per-grid IRLS counts, {position: u} of the
     positions in `keep_out` copied to the host, per-grid column paths).  `flags` are extra
@@ -824,6 +830,17 @@ def stack_measure(phases, weights, warmup, steps, world, local, npx_all, flags=0
     iters = [sts[k].irls_iters for k in range(n)]
     paths = [sts[k].col_path for k in range(n)]
     outs = {k: keep[4 * k + 2].cpu().numpy() for k in keep_out if k < n}
+    if profile_out is not None and n:
+        # one more solve with every launch bracketed by CUDA events (groups one after
+        # another); the sums of grid 0's stats cover all groups
+        prm.flags |= _lib.UNW_F_PROFILE
+        solve()
+        torch.cuda.synchronize()
+        st0 = sts[0]
+        for i, name in enumerate(_lib.PROF_NAMES):
+            if st0.prof_launches[i]:
+                profile_out[name] = {"launches": int(st0.prof_launches[i]), "ms_total": round(float(st0.prof_ms[i]), 3),
+                                     "us_per_launch": round(float(st0.prof_ms[i]) * 1e3 / st0.prof_launches[i], 2)}
     del keep, ws
     torch.cuda.empty_cache()
     return npx_all * steps / 1e6 / t, t / steps, iters, outs, paths

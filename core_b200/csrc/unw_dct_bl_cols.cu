@@ -41,12 +41,16 @@ __global__ void __launch_bounds__(BL::T * NSEQ, bl_min_blocks<BL::T * NSEQ>()) k
     for (int slab = local; slab < nslab; slab += nct) {
         const int ja = 2 * NSEQ * slab + 2 * s;
         const bool hasa = ja < W, hasb = ja + 1 < W;
+        // the pair as one 8-byte access (ja is even): one L1 request per row instead of two
+        // (column pass 392.8 vs 439.6 us at 2436 x 5911, 147.6 vs 160.3 at 1838 x 4122, same bits)
+        const bool vec = hasb && !(P & 1);
         __syncthreads();  // previous slab's reads of sm are done
         // column pair (ja, ja+1): row i goes to DFT position perm(i)
         for (int i = t; i < H; i += T) {
             const float* a = Tm + (size_t)i * P + ja;
             float2 x = make_float2(0.f, 0.f);
-            if (hasb) x = make_float2(a[0], a[1]);
+            if (vec) x = *reinterpret_cast<const float2*>(a);
+            else if (hasb) x = make_float2(a[0], a[1]);
             else if (hasa) x.x = a[0];
             sms[BL::pos(mk_perm(i, H))] = x;
         }
@@ -69,7 +73,8 @@ __global__ void __launch_bounds__(BL::T * NSEQ, bl_min_blocks<BL::T * NSEQ>()) k
         for (int i = t; i < H; i += T) {
             const float2 v = sms[BL::pos(mk_perm(i, H))];
             float* a = Tm + (size_t)i * P + ja;
-            if (hasb) { a[0] = v.x; a[1] = -v.y; }
+            if (vec) *reinterpret_cast<float2*>(a) = make_float2(v.x, -v.y);
+            else if (hasb) { a[0] = v.x; a[1] = -v.y; }
             else if (hasa) a[0] = v.x;
         }
     }
