@@ -29,6 +29,7 @@ UNW_F_COL_TC = 32
 UNW_F_COL_FFT = 64
 UNW_F_COL_NO_TMA = 128
 UNW_F_COL_TMA = 256
+UNW_F_MV_NO_TMA = 512
 
 PROF_NAMES = ["bbox", "setup", "row_rho", "col", "row_inv", "matvec", "row_upd", "row_r0", "head", "elem", "post"]
 PROF_N = len(PROF_NAMES)

@@ -156,7 +156,7 @@ struct GridLayout {
 
 struct BatchLayout {
     size_t rowany, colany, bbox, gdev, starts;
-    size_t tcmaps;           // two 128-byte tensor maps per grid (tensor-core column pass)
+    size_t tcmaps;           // UNW_MAPS_PER_GRID 128-byte tensor maps per grid (TMA-staged passes)
     std::vector<size_t> base;
     std::vector<GridLayout> g;
     size_t total;
@@ -223,7 +223,7 @@ BatchLayout batch_layout(int n, const long long* H, const long long* W) {
     B.bbox = take(sizeof(int) * 4 * (size_t)n);
     B.gdev = take(sizeof(GridDev) * (size_t)n);
     B.starts = take(sizeof(int) * (size_t)(KS_NKIND + 1) * (2 * (size_t)n + 1));
-    B.tcmaps = take(256 * (size_t)n);
+    B.tcmaps = take(UNW_MAP_BYTES * (size_t)n);
     for (int g = 0; g < n; g++) {
         GridLayout L = grid_layout(H[g], W[g]);
         B.base.push_back(o);
@@ -243,6 +243,7 @@ struct Shape {
     int row_bl = 0, col_bl = 0;   // Bluestein register-FFT paths (FFT length M), 0 = not used
     int col_tc = 0;               // tensor-core column pass (mixed precision), chosen by the autotuner
     int col_p2_tma = 0;           // power-of-two column pass with the slab moved by TMA (H 2048 / 4096)
+    int mv_tma = 0;               // matvec on TMA-staged halo tiles
 };
 
 int elem_ctas(long long npx) {
@@ -310,7 +311,12 @@ struct Solver {
     int* dstarts = nullptr;
     Shape sh;
     TcMaps maps;                 // tensor maps of the split DCT matrices (col_tc)
-    void* bmaps = nullptr;       // device: per-grid tensor maps of the pass's float32 sources
+    void* bmaps = nullptr;       // device: per-grid tensor maps of the TMA-staged passes
+    std::vector<unsigned char> hmaps;  // their host image (UNW_MAP_BYTES per grid, 64-byte aligned)
+    unsigned char* host_maps(int ngrids) {
+        if (hmaps.size() < UNW_MAP_BYTES * (size_t)ngrids + 64) hmaps.assign(UNW_MAP_BYTES * (size_t)ngrids + 64, 0);
+        return (unsigned char*)(((size_t)hmaps.data() + 63) & ~(size_t)63);
+    }
     TuneResult tune;             // autotuner timings of the column pass (mixed precision)
     UnwScalars sc{};
     const int* ds(int kind) const { return dstarts + (size_t)kind * (n + 1); }
@@ -387,7 +393,9 @@ int enqueue_pcg(Solver& S, int t, int k0, int k1) {
     const int n = S.n;
     cudaStream_t s = S.s;
     for (int k = k0; k < k1; k++) {
-        PL(UNW_PROF_MATVEC, unw_launch_simple(UNW_K_MATVEC, S.total[KS_MATVEC], s, S.dg, S.ds(KS_MATVEC), n, k, S.sc));
+        PL(UNW_PROF_MATVEC, S.sh.mv_tma ? unw_launch_matvec_tma(S.total[KS_MATVEC], s, S.dg, S.ds(KS_MATVEC), n, S.bmaps)
+                                        : unw_launch_simple(UNW_K_MATVEC, S.total[KS_MATVEC], s, S.dg, S.ds(KS_MATVEC),
+                                                            n, k, S.sc));
         PL(UNW_PROF_ROW_UPD, L_rowf(S, 2, t, k));
         PL(UNW_PROF_COL, L_col(S, 2));
         PL(UNW_PROF_ROW_INV, L_rowi(S, 2));
@@ -778,14 +786,14 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
         cudaError_t te = B.g[idx[0]].tc ? unw_tc_prepare(tc_h, tab, &S.maps, s) : cudaErrorInvalidValue;
         if (te == cudaSuccess) {
             // per-grid tensor maps of T and p1 (the pass's float32 sources), 64-byte aligned
-            std::vector<unsigned char> hm(256 * (size_t)n + 64);
-            unsigned char* h = (unsigned char*)up((size_t)hm.data(), 64);
+            unsigned char* h = S.host_maps(n);
             for (int g = 0; g < n && te == cudaSuccess; g++) {
                 const GridDev& G = S.hg[g];
-                if (G.H > 0 && !unw_tc_data_maps(G.T, G.p1, G.H, G.W, G.P, h + 256 * (size_t)g)) te = cudaErrorNotSupported;
+                if (G.H > 0 && !unw_tc_data_maps(G.T, G.p1, G.H, G.W, G.P, h + UNW_MAP_BYTES * (size_t)g))
+                    te = cudaErrorNotSupported;
             }
-            S.bmaps = base + B.tcmaps + 256 * (size_t)slot;
-            if (te == cudaSuccess) te = cudaMemcpyAsync(S.bmaps, h, 256 * (size_t)n, cudaMemcpyHostToDevice, s);
+            S.bmaps = base + B.tcmaps + UNW_MAP_BYTES * (size_t)slot;
+            if (te == cudaSuccess) te = cudaMemcpyAsync(S.bmaps, h, UNW_MAP_BYTES * (size_t)n, cudaMemcpyHostToDevice, s);
         }
         if (te == cudaSuccess) {
             if (prm->flags & UNW_F_COL_TC) {
@@ -804,24 +812,41 @@ int prepare(Solver& S, const std::vector<int>& idx, const unw_grid* grids, const
     // covers H <= 1024 only)
     S.sh.col_p2_tma = 0;
     if (!S.sh.col_tc && S.sh.col_p2 && unw_p2_tma_nseq(S.sh.col_p2) > 0 && !(prm->flags & UNW_F_COL_NO_TMA)) {
-        std::vector<unsigned char> hm(256 * (size_t)n + 64);
-        unsigned char* h = (unsigned char*)up((size_t)hm.data(), 64);
+        unsigned char* h = S.host_maps(n);
         bool ok = true;
         for (int g = 0; g < n && ok; g++) {
             const GridDev& G = S.hg[g];
             if (G.H > 0)
                 ok = G.col_nseq == unw_p2_tma_nseq(S.sh.col_p2) &&
-                     unw_p2_tma_maps(G.T, G.H, G.W, G.P, G.col_nseq, h + 256 * (size_t)g);
+                     unw_p2_tma_maps(G.T, G.H, G.W, G.P, G.col_nseq,
+                                     h + UNW_MAP_BYTES * (size_t)g + 128 * UNW_MAP_COL);
         }
         if (ok) {
-            S.bmaps = base + B.tcmaps + 256 * (size_t)slot;
-            CK(cudaMemcpyAsync(S.bmaps, h, 256 * (size_t)n, cudaMemcpyHostToDevice, s));
+            S.bmaps = base + B.tcmaps + UNW_MAP_BYTES * (size_t)slot;
+            CK(cudaMemcpyAsync(S.bmaps, h, UNW_MAP_BYTES * (size_t)n, cudaMemcpyHostToDevice, s));
             S.sh.col_p2_tma = 1;
             if (!(prm->flags & UNW_F_COL_TMA)) {
                 int Wsum = 0;
                 for (int g = 0; g < n; g++) Wsum += S.hg[g].W;
                 S.sh.col_p2_tma = autotune_tma(S, S.sh.col_p2, Wsum);
             }
+        }
+    }
+    // matvec on TMA-staged halo tiles: per-grid maps of p, wIx and wIy in the grid's map slot
+    S.sh.mv_tma = 0;
+    if (!(prm->flags & UNW_F_MV_NO_TMA)) {
+        unsigned char* h = S.host_maps(n);
+        bool ok = true;
+        for (int g = 0; g < n && ok; g++) {
+            const GridDev& G = S.hg[g];
+            if (G.H > 0)
+                ok = unw_mv_tma_maps(G.p0, G.wIx, G.wIy, G.H, G.W, G.P,
+                                     h + UNW_MAP_BYTES * (size_t)g + 128 * UNW_MAP_MV);
+        }
+        if (ok) {
+            S.bmaps = base + B.tcmaps + UNW_MAP_BYTES * (size_t)slot;
+            CK(cudaMemcpyAsync(S.bmaps, h, UNW_MAP_BYTES * (size_t)n, cudaMemcpyHostToDevice, s));
+            S.sh.mv_tma = 1;
         }
     }
     bool any_grid = false;

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, ct_min_blocks<N / 16 * NSEQ>())
     const int s = threadIdx.x % NSEQ, t = threadIdx.x / NSEQ;
     unsigned char* const base = (unsigned char*)(((size_t)ct_raw + 127) & ~(size_t)127);
     float2* sms = reinterpret_cast<float2*>(base) + s * RegFft<N>::SEQ_STRIDE;
-    const CUtensorMap* me = maps + 2 * g;  // even rows of T
+    const CUtensorMap* me = maps + UNW_MAPS_PER_GRID * g + UNW_MAP_COL;  // even rows of T
     const CUtensorMap* mo = me + 1;        // odd rows of T
     const float2* __restrict__ tw = G.pcol.fft.tw;
     const float2* __restrict__ dw = G.pcol.dctw;
@@ -209,7 +209,7 @@ cudaError_t ct_launch(int mode, int nblk, cudaStream_t s, const GridDev* gd, con
     constexpr int NS = ct_nseq<N>();
     const size_t smem = sizeof(float2) * RegFft<N>::SEQ_STRIDE * NS + 128;
     auto go = [&](auto kfn) {
-        const cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const cudaError_t e = unw_smem_limit((const void*)kfn);
         if (e != cudaSuccess) return e;
         kfn<<<nblk, N / 16 * NS, smem, s>>>(gd, st, n, maps);
         return cudaGetLastError();

@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_col_tc(const GridDev* __restr
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     unsigned char* smem = (unsigned char*)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
     // the float32 source of B: T (first product) or Y in p1 (second), one map per grid
-    const CUtensorMap* bmap = bmaps + 2 * g + EPI;
+    const CUtensorMap* bmap = bmaps + UNW_MAPS_PER_GRID * g + UNW_MAP_COL + EPI;
 
     if (tid == 0) {
         for (int s = 0; s < TC_STAGES; s++) {

@@ -128,7 +128,18 @@ enum {
 cudaError_t unw_launch_post(int which, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,
                             int n, const UnwScalars& sc, const GridDev* host_grids);
 
-// power-of-two column pass with the slab moved by TMA (unw_dct_p2_tma.cu), H = 4096
+// Per-grid tensor maps of the TMA-staged passes (one 128-byte CUtensorMap each): the
+// column pass's two (tensor-core T / p1, or power-of-two even / odd rows of T) at
+// UNW_MAP_COL, the matvec's three (p, wIx, wIy) at UNW_MAP_MV.
+#define UNW_MAPS_PER_GRID 8
+#define UNW_MAP_BYTES (128 * UNW_MAPS_PER_GRID)
+#define UNW_MAP_COL 0
+#define UNW_MAP_MV 2
+bool unw_mv_tma_maps(const float* p, const float* wIx, const float* wIy, int H, int W, int P, void* out);
+cudaError_t unw_launch_matvec_tma(int nblk, cudaStream_t s, const GridDev* gd, const int* starts, int n,
+                                  const void* maps);
+
+// power-of-two column pass with the slab moved by TMA (unw_dct_p2_tma.cu), H = 2048 / 4096
 int unw_p2_tma_nseq(int N);
 bool unw_p2_tma_maps(const float* T, int H, int W, int P, int nseq, void* out);
 cudaError_t unw_launch_col_p2_tma(int N, int mode, int nblk, cudaStream_t s, const GridDev* gd, const int* starts,

@@ -116,6 +116,20 @@ __device__ __forceinline__ void rowfwd_finalize(InstState* st, const double (&ac
     }
 }
 
+// Last CTA of the matvec: pAp and its scalar step (utils_unwrap2d.py:1433-1442): stop on a tiny
+// or non-finite pAp, else alpha = rz / pAp clamped to [-1e6, 1e6].
+__device__ __forceinline__ void matvec_finalize(InstState* st, double pAp) {
+    st->pAp = pAp;
+    st->cg_iter += 1;
+    if (fabs(pAp) < 1e-15 || !isfinite(pAp)) {
+        st->cg_active = 0;
+    } else {
+        double a = st->rz / pAp;
+        a = a < -1e6 ? -1e6 : (a > 1e6 ? 1e6 : a);
+        st->alpha = (float)a;
+    }
+}
+
 // Row-inverse modes:
 //  0 INITU u = nan_to_num(z) (utils_unwrap2d.py:1498-1502), sum of u * valid
 //  1 P0    p = z = M^-1 r                     (utils_unwrap2d.py:1421-1424)

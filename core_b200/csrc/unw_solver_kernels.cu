@@ -430,18 +430,7 @@ __global__ void __launch_bounds__(512, 2) k_matvec(const GridDev* __restrict__ g
     }
     if (arrive<1>(G, local, nct, acc, red)) {
         finish_sum<1>(G, nct, acc, red);
-        if (threadIdx.x == 0) {
-            const double pAp = acc[0];
-            st->pAp = pAp;
-            st->cg_iter += 1;
-            if (fabs(pAp) < 1e-15 || !isfinite(pAp)) {
-                st->cg_active = 0;
-            } else {
-                double a = st->rz / pAp;
-                a = a < -1e6 ? -1e6 : (a > 1e6 ? 1e6 : a);
-                st->alpha = (float)a;
-            }
-        }
+        if (threadIdx.x == 0) matvec_finalize(st, acc[0]);
     }
 }
 

@@ -74,6 +74,8 @@ typedef struct unw_params {
                                same arithmetic and bits); by default an autotuner times both
                                per shape on the first call and keeps the faster               */
 #define UNW_F_COL_TMA 256    /* always the TMA-staged column pass where it applies           */
+#define UNW_F_MV_NO_TMA 512  /* matvec with plain loads instead of TMA-staged halo tiles (the
+                               same arithmetic and bits; for comparison)                     */
 
 /* Kernel families timed under UNW_F_PROFILE (index into unw_stats.prof_*). */
 enum {

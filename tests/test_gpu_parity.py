@@ -471,6 +471,20 @@ def test_tma_column_pass_equals_plain_loads(shape):
     assert not s1["status"] & _lib.UNW_S_TC_TIMEOUT
 
 
+@pytest.mark.parametrize("shape", [(256, 256), (200, 131), (37, 50), (1, 7), (17, 4097), (1025, 2000)])
+def test_tma_matvec_equals_plain_loads(shape):
+    # the matvec runs on TMA-staged halo tiles unless UNW_F_MV_NO_TMA is set; the tiles, the
+    # thread mapping and the arithmetic are those of the plain-load kernel, so both must give
+    # identical bits (widths that are not multiples of four exercise the pitch columns)
+    p, c, _ = gen_g2(*shape, seed=13)
+    u1, c1, s1 = _solve_flags(p, c, 0)
+    u2, c2, s2 = _solve_flags(p, c, _lib.UNW_F_MV_NO_TMA)
+    np.testing.assert_array_equal(u1.view(np.uint32), u2.view(np.uint32))
+    np.testing.assert_array_equal(c1, c2)
+    assert s1["irls_iters"] == s2["irls_iters"] and s1["cg_iters_total"] == s2["cg_iters_total"]
+    assert not s1["status"] & _lib.UNW_S_TC_TIMEOUT
+
+
 def test_fixed_iters_runs_every_iteration():
     # tol = cg_tol = 0: only the numerical breaks can end an iteration early
     from oracle.irls_oracle import OracleStats
