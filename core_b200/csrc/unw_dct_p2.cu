@@ -122,12 +122,28 @@ __global__ void __launch_bounds__(N / 16, (rowf_blocks<N / 16, MODE>())) k_rowf_
     const int i0 = 2 * pair, i1 = i0 + 1;
     const bool has1 = i1 < H;
     __syncthreads();  // previous row pair's reads of sm are done
-    for (int c4 = t; c4 < N / 4; c4 += T) {
-        const int j = 4 * c4;
-        const float4 a = rowf_vals4<MODE>(G, U, Lo, pk, alpha, i0, j, acc);
-        const float4 b = has1 ? rowf_vals4<MODE>(G, U, Lo, pk, alpha, i1, j, acc) : make_float4(0.f, 0.f, 0.f, 0.f);
+#ifndef UNW_ROWF_UNROLL
+#define UNW_ROWF_UNROLL 1
+#endif
+    if (MODE == 2 && UNW_ROWF_UNROLL) {
+        // the thread's four 16-byte groups per row as one unrolled sequence (a fixed trip
+        // count), so that the loads of later groups can be issued before earlier ones are used
 #pragma unroll
-        for (int c = 0; c < 4; c++) sm[pad16(mk_pos(j + c, N))] = make_float2(f4get(a, c), f4get(b, c));
+        for (int m = 0; m < N / (4 * T); m++) {
+            const int j = 4 * (t + m * T);
+            const float4 a = rowf_vals4<MODE>(G, U, Lo, pk, alpha, i0, j, acc);
+            const float4 b = has1 ? rowf_vals4<MODE>(G, U, Lo, pk, alpha, i1, j, acc) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int c = 0; c < 4; c++) sm[pad16(mk_pos(j + c, N))] = make_float2(f4get(a, c), f4get(b, c));
+        }
+    } else {
+        for (int c4 = t; c4 < N / 4; c4 += T) {
+            const int j = 4 * c4;
+            const float4 a = rowf_vals4<MODE>(G, U, Lo, pk, alpha, i0, j, acc);
+            const float4 b = has1 ? rowf_vals4<MODE>(G, U, Lo, pk, alpha, i1, j, acc) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int c = 0; c < 4; c++) sm[pad16(mk_pos(j + c, N))] = make_float2(f4get(a, c), f4get(b, c));
+        }
     }
     __syncthreads();
     smem_fft<N>(sm, t, G.prow.fft.tw);
