@@ -203,6 +203,12 @@ __device__ __forceinline__ void rowi_store4(const GridDev& G, int i, int j, floa
 #ifndef UNW_ROWI_STAGED
 #define UNW_ROWI_STAGED 1
 #endif
+#ifndef UNW_ROWI_REGIN
+#define UNW_ROWI_REGIN 1
+#endif
+#ifndef UNW_ROWI_QB
+#define UNW_ROWI_QB 4
+#endif
 template <int N, int MODE>
 __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const GridDev* __restrict__ grids,
                                                                          const int* __restrict__ starts, int n) {
@@ -233,6 +239,35 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
             if (has1) asm volatile("prefetch.global.L2 [%0];" ::"l"(ra + P + c));
         }
     }
+    if constexpr (UNW_ROWI_REGIN && MODE == 2) {
+    // DCT-III pre-twiddle formed straight into the register layout of the FFT's first pass:
+    // thread t holds k = t + T q (q = 0..15) and reads Y_k and its mirror Y_{N-k} of both rows
+    // (each a coalesced warp-wide run of the row), V'_k = conj(w_k) (Y_k - i Y_{N-k}), Y_N = 0;
+    // v[q] = conj(C'_k).  Same arithmetic per element as the staged form below.
+    float2 v[16];
+#pragma unroll
+    for (int h = 0; h < 16 / UNW_ROWI_QB; h++) {
+        float ya[UNW_ROWI_QB], yam[UNW_ROWI_QB], yb[UNW_ROWI_QB], ybm[UNW_ROWI_QB];
+#pragma unroll
+        for (int e = 0; e < UNW_ROWI_QB; e++) {
+            const int k = t + (UNW_ROWI_QB * h + e) * T;
+            ya[e] = Ta[k];
+            yam[e] = k ? Ta[N - k] : 0.f;
+            yb[e] = has1 ? Tb[k] : 0.f;
+            ybm[e] = (has1 && k) ? Tb[N - k] : 0.f;
+        }
+#pragma unroll
+        for (int e = 0; e < UNW_ROWI_QB; e++) {
+            const int k = t + (UNW_ROWI_QB * h + e) * T;
+            const float2 wk = cconj(__ldg(&dw[k]));
+            const float2 Pa = cmul(wk, make_float2(ya[e], -yam[e]));
+            const float2 Pb = cmul(wk, make_float2(yb[e], -ybm[e]));
+            v[UNW_ROWI_QB * h + e] = cconj(make_float2(Pa.x - Pb.y, Pa.y + Pb.x));
+        }
+    }
+    __syncthreads();  // previous row pair's reads of sm are done
+    io_fft<N, true, false>(v, sm, t, G.prow.fft.tw);
+    } else {
 #if UNW_ROWI_STAGED
     // the row pair's T values: all eight 16-byte loads of a thread issued together, then
     // (Y_a[k], Y_b[k]) into sm[pad16(k)]
@@ -295,6 +330,7 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
 #endif
     __syncthreads();
     smem_fft<N>(sm, t, G.prow.fft.tw);
+    }
 #if UNW_ROWI_STAGED
     if (MODE == 2) {
         // p = z + beta p: the thread's p loads (L2-prefetched above) all issued before the

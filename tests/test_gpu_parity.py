@@ -515,3 +515,18 @@ def test_long_axes_solve_matches_oracle(shape):
     rms = lambda a: float(np.sqrt(np.mean((a - a.mean()) ** 2)))
     spread = rms((u32.astype(np.float64) - u64)[v])
     _compare(u, cc, u64, cc64, p, tol_rms=max(1e-3, 5 * spread))
+
+
+@pytest.mark.parametrize("shape", [(129, 1024), (255, 4096), (1, 2048), (3, 8192), (1023, 512)])
+def test_odd_row_count_on_power_of_two_rows_matches_oracle(shape):
+    # power-of-two rows run on the register-FFT row passes two rows at a time; an odd row
+    # count leaves the last row without a partner (its imaginary half is zero)
+    p, c, _ = gen_g1(*shape, seed=23)
+    kw = dict(max_iter=3, cg_max_iter=8)
+    u, cc = core_b200.irls_unwrap_2d(p, c, **kw)
+    u64, cc64 = oracle_unwrap(p, c, dtype=np.float64, **kw)
+    u32, _ = oracle_unwrap(p, c, **kw)
+    v = np.isfinite(p)
+    rms = lambda a: float(np.sqrt(np.mean((a - a.mean()) ** 2)))
+    spread = rms((u32.astype(np.float64) - u64)[v])
+    _compare(u, cc, u64, cc64, p, tol_rms=max(1e-3, 5 * spread))
