@@ -12,6 +12,7 @@
 // scaling, DCT-III pre-twiddle), inverse FFT, store.
 #include "unw_regfft.cuh"
 #include "unw_rowops.cuh"
+#include "unw_colspec.cuh"
 #include "unw_kernels.h"
 
 template <int T>
@@ -425,16 +426,7 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, min_blocks<N / 16 * NSEQ>()) k_
     __syncthreads();  // previous slab's reads of sm are done
     io_fft<N, true, false>(v, sms, t, tw);
     const float ca = hasa ? G.sW[ja] : 1.0f, cb = hasb ? G.sW[ja + 1] : 1.0f;
-    for (int k = t; k <= N / 2; k += T) {
-        const int km = (N - k) & (N - 1);
-        const float2 C = sms[pad16(k)], Cm = sms[pad16(km)];
-        const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
-        const float ck = __ldg(&sH[k]), cm = __ldg(&sH[km]);
-        float2 ok, om;
-        col_spectral_pair<(MODE >= 1)>(C, Cm, k, km, wk, wm, ck, cm, ca, cb, ja == 0, hasb, negs, ok, om, acc[0]);
-        if (km != k) sms[pad16(km)] = om;
-        sms[pad16(k)] = ok;
-    }
+    col_spectral_p2<N, MODE>(sms, t, dw, sH, ca, cb, ja == 0, hasb, negs, acc[0]);
     __syncthreads();
     io_fft<N, false, true>(v, sms, t, tw);
 #pragma unroll

@@ -29,6 +29,7 @@
 #include "unw_kernels.h"
 #include "unw_regfft.cuh"
 #include "unw_rowops.cuh"
+#include "unw_colspec.cuh"
 
 namespace {
 
@@ -148,17 +149,7 @@ __global__ void __launch_bounds__(N / 16 * NSEQ, ct_min_blocks<N / 16 * NSEQ>())
         __syncthreads();  // every staged read done before the transform writes the buffer
         io_fft<N, true, false>(v, sms, t, tw);
         const float ca = hasa ? G.sW[ja] : 1.0f, cb = hasb ? G.sW[ja + 1] : 1.0f;
-        for (int k = t; k <= N / 2; k += T) {
-            const int km = (N - k) & (N - 1);
-            const float2 C = sms[pad16(k)], Cm = sms[pad16(km)];
-            const float2 wk = __ldg(&dw[k]), wm = __ldg(&dw[km]);
-            const float ck = __ldg(&sH[k]), cm = __ldg(&sH[km]);
-            float2 ok2, om;
-            col_spectral_pair<(MODE >= 1)>(C, Cm, k, km, wk, wm, ck, cm, ca, cb, ja == 0, hasb, negs, ok2, om,
-                                           acc[0]);
-            if (km != k) sms[pad16(km)] = om;
-            sms[pad16(k)] = ok2;
-        }
+        col_spectral_p2<N, MODE>(sms, t, dw, sH, ca, cb, ja == 0, hasb, negs, acc[0]);
         __syncthreads();
         io_fft<N, false, true>(v, sms, t, tw);
         __syncthreads();  // every transform read of the buffer done before the slab is staged back
