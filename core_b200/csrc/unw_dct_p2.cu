@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
     smem_fft<N>(sm, t, G.prow.fft.tw);
     }
 #if UNW_ROWI_STAGED
-    if (MODE == 2) {
+    if constexpr (MODE == 2) {
         // p = z + beta p: the thread's p loads (L2-prefetched above) all issued before the
         // first use
         float4 pa[N / (4 * T)], pb[N / (4 * T)];
@@ -357,20 +357,21 @@ __global__ void __launch_bounds__(N / 16, min_blocks<N / 16>()) k_rowi_p2(const 
             st4f(G.p0, o, make_float4(za[0], za[1], za[2], za[3]));
             if (has1) st4f(G.p0, o + P, make_float4(zb[0], zb[1], zb[2], zb[3]));
         }
-        continue;
-    }
+    } else
 #endif
-    for (int c4 = t; c4 < N / 4; c4 += T) {
-        const int j = 4 * c4;
-        float za[4], zb[4];
+    {
+        for (int c4 = t; c4 < N / 4; c4 += T) {
+            const int j = 4 * c4;
+            float za[4], zb[4];
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const float2 v = sm[pad16(mk_pos(j + c, N))];
-            za[c] = v.x;
-            zb[c] = -v.y;
+            for (int c = 0; c < 4; c++) {
+                const float2 v = sm[pad16(mk_pos(j + c, N))];
+                za[c] = v.x;
+                zb[c] = -v.y;
+            }
+            rowi_store4<MODE>(G, i0, j, make_float4(za[0], za[1], za[2], za[3]), beta, acc);
+            if (has1) rowi_store4<MODE>(G, i1, j, make_float4(zb[0], zb[1], zb[2], zb[3]), beta, acc);
         }
-        rowi_store4<MODE>(G, i0, j, make_float4(za[0], za[1], za[2], za[3]), beta, acc);
-        if (has1) rowi_store4<MODE>(G, i1, j, make_float4(zb[0], zb[1], zb[2], zb[3]), beta, acc);
     }
     }
     if (MODE != 0) return;

@@ -423,18 +423,10 @@ __device__ double pseg(unsigned p, unsigned a, unsigned b) {
     return fabs((double)cr) / sqrt((double)L2);
 }
 
-__device__ double hull_dist(const unsigned* P, int m, const unsigned* Q, int n) {
-    if (!separated(P, m, Q, n) && !separated(Q, n, P, m)) return 0.0;
-    double d = INFINITY;
-    for (int i = 0; i < m; i++)
-        for (int k = 0; k < n; k++) d = fmin(d, pseg(P[i], Q[k], Q[k + 1 == n ? 0 : k + 1]));
-    for (int i = 0; i < n; i++)
-        for (int k = 0; k < m; k++) d = fmin(d, pseg(Q[i], P[k], P[k + 1 == m ? 0 : k + 1]));
-    return d;
-}
-
-// The same distance with the 32 lanes of a warp sharing the edge and vertex
-// loops (all lanes call it with the same arguments and get the same result).
+// Distance between two convex hulls P (m vertices) and Q (n vertices): 0 when no edge of either
+// separates them, else the smallest distance from a vertex of one to an edge of the other.  The
+// 32 lanes of a warp share the edge and vertex loops (all lanes call it with the same arguments
+// and get the same result).
 __device__ bool warp_separated(const unsigned* P, int m, const unsigned* Q, int n) {
     bool found = false;
     for (int k0 = 0; k0 < m && !found; k0 += 32) {
