@@ -364,7 +364,8 @@ def run_b200(args):
     t_prof = ev0.elapsed_time(ev1) / 1e3 / prof_steps
 
     # ---- end to end through the public API as a numpy caller uses it: numpy (pageable)
-    # input copied to the device and numpy output copied back inside the timed region
+    # input copied to the device (through the API's pinned staging) and numpy output copied
+    # back inside the timed region
     # warm-up in the timed loop's own pattern: a caller that keeps the previous
     # result while the next call runs holds two pinned output blocks
     pkw = dict(precision=args.precision, col_pass=args.col_pass)
@@ -515,7 +516,8 @@ def run_b200(args):
            "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": int(npx * 8),
                    "d2h_bytes_per_step": int(npx * 6),
                    "path": "core_b200.irls_unwrap_2d(numpy phase, numpy weight) -> numpy (u, conncomp); "
-                           "pageable host input, pinned staging for the output"},
+                           "pageable numpy input sent through chunked pinned staging, pinned staging "
+                           "for the output"},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches // 1,
            "stack": stack, "link": link, "accuracy": accuracy, "mixed": mixed,
            "mixed_1024": mixed_small(local) if not args.no_mixed_small else None,

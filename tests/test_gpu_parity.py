@@ -373,6 +373,30 @@ def test_float64_and_noncontiguous_inputs():
     _compare(u1, c1, u2, c2, p, tol_rms=1e-5)
 
 
+def test_large_host_inputs_equal_device_inputs():
+    # host arrays of 4 MB and more reach the device through chunked pinned staging (more than
+    # one chunk here, the last one partial); the solve must see exactly the CUDA tensor's data
+    p, c, _ = gen_g1(1500, 1601, seed=29)
+    p = p.copy()
+    p[7, 9] = np.nan
+    c = c.copy()
+    c[11, 13] = np.nan
+    kw = dict(max_iter=2, cg_max_iter=5)
+    ud, cd = core_b200.irls_unwrap_2d(torch.from_numpy(p).cuda(), torch.from_numpy(c).cuda(), **kw)
+    ud = ud.cpu().numpy()
+    cd = cd.cpu().numpy().view(np.uint16)
+    big = np.full((1600, 1700), np.nan)
+    big[50:1550, 40:1641] = p
+    for ph, wt in [(p, c), (p.astype(np.float64), c.astype(np.float64)), (big[50:1550, 40:1641], c),
+                   (torch.from_numpy(p), torch.from_numpy(c))]:
+        u, cc = core_b200.irls_unwrap_2d(ph, wt, **kw)
+        if isinstance(u, torch.Tensor):
+            u = u.cpu().numpy()
+            cc = cc.cpu().numpy().view(np.uint16)
+        assert np.array_equal(u, ud, equal_nan=True)
+        assert np.array_equal(cc, cd)
+
+
 def test_torch_cuda_input_returns_device_tensors():
     p, c, _ = gen_g1(64, 64, seed=9)
     pt = torch.from_numpy(p).to(DEV)
