@@ -10,7 +10,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import _lib
-from .irls import _torch, resolve_device
+from .irls import _np_to_device, _torch, resolve_device
 
 
 def goldstein(phase, corr, psize_y=32, psize_x=None, threshold=0.5, device='auto'):
@@ -37,8 +37,8 @@ def goldstein(phase, corr, psize_y=32, psize_x=None, threshold=0.5, device='auto
             ph = phase.to(device=dev, dtype=torch.complex64).contiguous()
             cr = corr.to(device=dev, dtype=torch.float32).contiguous()
         else:
-            ph = torch.from_numpy(np.ascontiguousarray(phase, np.complex64)).to(dev)
-            cr = torch.from_numpy(np.ascontiguousarray(corr, np.float32)).to(dev)
+            ph = _np_to_device(np.ascontiguousarray(phase, np.complex64), dev)
+            cr = _np_to_device(np.ascontiguousarray(corr, np.float32), dev)
         out = torch.empty((H, W), dtype=torch.complex64, device=dev)
         nb = lib.unw_goldstein_workspace_bytes(H, W, psize_y, psize_x)
         if nb == 0:

@@ -35,7 +35,7 @@ import time
 import numpy as np
 
 from . import _lib
-from .irls import _torch, resolve_device
+from .irls import _np_to_device, _torch, resolve_device
 
 
 class _LinkWorkspace:
@@ -115,7 +115,7 @@ def _device_labels(conncomp, dev, H, W):
             if a.size and (a.max() > 65535 or a.min() < 0):
                 raise ValueError("conncomp labels must lie in [0, 65535]")
             a = a.astype(np.uint16)
-        t = torch.from_numpy(np.ascontiguousarray(a).view(np.int16)).to(dev)
+        t = _np_to_device(np.ascontiguousarray(a).view(np.int16), dev)
     if tuple(t.shape) != (H, W):
         raise ValueError(f"conncomp shape {tuple(t.shape)} differs from phase shape {(H, W)}")
     return t
@@ -207,7 +207,7 @@ def link_components(phase, conncomp=None, conncomp_size=100, conncomp_gap=None, 
             ph = ph2.to(device=dev, dtype=torch.float32,
                         non_blocking=ph2.device.type == "cpu" and ph2.is_pinned()).contiguous()
         else:
-            ph = torch.from_numpy(np.ascontiguousarray(ph2, dtype=np.float32)).to(dev)
+            ph = _np_to_device(np.ascontiguousarray(ph2, dtype=np.float32), dev)
         if bool(torch.isnan(ph).all()):
             return finish(ph.clone())
         lab = _device_labels(cc2, dev, H, W) if cc2 is not None else None
@@ -306,8 +306,8 @@ def find_component_connections_fast(labeled_array, phase, components, conncomp_g
     ph2 = np.asarray(phase, np.float32)
     dev = resolve_device(device, None)
     with torch.cuda.device(dev):
-        ph = torch.from_numpy(np.ascontiguousarray(ph2)).to(dev)
-        lab = torch.from_numpy(np.ascontiguousarray(lab16).view(np.int16)).to(dev)
+        ph = _np_to_device(np.ascontiguousarray(ph2), dev)
+        lab = _np_to_device(np.ascontiguousarray(lab16).view(np.int16), dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
         _, _, pairs, npair, _ = _device_pairs(ph, lab, 1, int(max_neighbors), int(n_neighbors), dev, stream)
     return _greedy_connections(pairs, npair, int(max_neighbors), conncomp_gap)

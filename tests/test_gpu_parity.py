@@ -397,6 +397,27 @@ def test_large_host_inputs_equal_device_inputs():
         assert np.array_equal(cc, cd)
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.int16, np.complex64])
+def test_staged_host_copy_is_exact(dtype):
+    from core_b200.irls import _np_to_device
+    rng = np.random.default_rng(3)
+    n = 3 * (8 << 20) // np.dtype(dtype).itemsize + 12345      # three full chunks and a partial one
+    if dtype == np.int16:
+        a = rng.integers(-32768, 32767, n, dtype=np.int16)
+    elif dtype == np.complex64:
+        a = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    else:
+        a = rng.standard_normal(n).astype(np.float32)
+        a[::1001] = np.nan
+    a = a.reshape(-1, 5) if n % 5 == 0 else a
+    dev = torch.device("cuda", 0)
+    with torch.cuda.device(dev):
+        t = _np_to_device(a, dev)
+        torch.cuda.current_stream(dev).synchronize()
+    assert t.shape == a.shape and t.is_cuda
+    assert np.array_equal(t.cpu().numpy().view(np.uint8), a.view(np.uint8))
+
+
 def test_torch_cuda_input_returns_device_tensors():
     p, c, _ = gen_g1(64, 64, seed=9)
     pt = torch.from_numpy(p).to(DEV)
